@@ -1,0 +1,161 @@
+/* parex_b200 — B200-native random-walk expander decomposition, C ABI.
+ *
+ * Every entry point replaces one member of the reference's drop-in class
+ * CudaDeviceManager (cuda/interface.h:16-57); the reference member is named
+ * beside each declaration.  Plain pointers and sizes only: no CUDA, C++ or
+ * torch types cross this boundary.  Host buffers are ordinary host memory
+ * unless a function says otherwise.
+ *
+ * Threading: a handle is used by one host thread at a time.  All device work
+ * of a handle runs on the handle's stream, in call order.
+ * Errors: every function returns a pxr_status; pxr_last_error() gives the
+ * message of the last failure on that handle.
+ */
+#ifndef PAREX_B200_H
+#define PAREX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PXR_ABI_VERSION 1
+#define PXR_INVALID_EDGE 0xFFFFFFFFu   /* disabled CSR slot, lib/core/definitions.h:52 */
+
+typedef enum {
+    PXR_OK = 0,
+    PXR_INVALID_ARG = 1,     /* bad pointer, size or state                           */
+    PXR_OUT_OF_MEMORY = 2,   /* device allocation failed                              */
+    PXR_ITER_CAP = 3,        /* round cap reached before every cluster was certified  */
+    PXR_CUDA_ERROR = 4,      /* a CUDA runtime call failed                            */
+    PXR_DEVICE_FAULT = 5,    /* a device-side bounded wait or invariant check failed  */
+    PXR_NOT_INITIALIZED = 6  /* no graph uploaded yet                                 */
+} pxr_status;
+
+/* Division used for the sweep's sparsity ratio. */
+enum {
+    PXR_DIV_IEEE = 0,        /* correctly rounded float division (default)                */
+    PXR_DIV_REFERENCE = 1    /* the approximate division the reference's fast-math build
+                                uses; reproduces its tie-breaking on equal ratios        */
+};
+
+/* Round driver. */
+enum {
+    PXR_DRIVER_GRAPH = 0,    /* rounds replayed from a captured CUDA graph (default)      */
+    PXR_DRIVER_STREAM = 1    /* rounds launched kernel by kernel from the host            */
+};
+
+typedef struct {
+    uint32_t seed;           /* randSeed, lib/core/definitions.h:46 (6582)              */
+    float sc_threshold;      /* sweep sparsity threshold, definitions.h:50 (0.3)          */
+    float rw_threshold;      /* potential threshold, definitions.h:49 (1e-4)              */
+    uint32_t max_rounds;     /* MAX_NUM_ITER, cuda/device.h:371 (200000)                  */
+    int32_t device;          /* CUDA device ordinal                                       */
+    uint32_t division;       /* PXR_DIV_*                                                 */
+    uint32_t driver;         /* PXR_DRIVER_*                                              */
+    uint32_t reserved[9];
+} pxr_config;
+
+/* One sweep cut per active cluster: SweepCutData, lib/core/definitions.h:57-61. */
+typedef struct { int32_t label; float sparsity; uint32_t offset; } pxr_sweep_cut;
+
+/* Sweep order entry: NodeData, lib/core/definitions.h:68-78. */
+typedef struct {
+    uint32_t nix;
+    uint32_t prefix_volume;
+    int32_t prefix_edge_diff;
+    uint32_t offset_in_cluster;
+} pxr_node_data;
+
+typedef struct {
+    uint32_t rounds;             /* rounds run by the last pxr_decompose                 */
+    uint32_t active_vertices;    /* numActiveNodes                                        */
+    uint32_t active_clusters;    /* numActiveClusters                                     */
+    uint32_t clusters_with_cut;  /* numClustersWithCut of the last sweep                  */
+    uint64_t device_bytes;       /* device memory held by the handle                      */
+    double last_decompose_ms;    /* device time of the last pxr_decompose (CUDA events)    */
+} pxr_stats;
+
+void pxr_config_default(pxr_config* cfg);
+const char* pxr_status_string(pxr_status s);
+const char* pxr_last_error(const void* handle);
+
+typedef struct pxr_handle pxr_handle;
+
+/* CudaDeviceManager::CudaDeviceManager() (cuda/interface.h:18). */
+pxr_status pxr_create(const pxr_config* cfg, pxr_handle** out);
+/* CudaDeviceManager::~CudaDeviceManager() (cuda/interface.h:19). */
+void pxr_destroy(pxr_handle* h);
+
+/* Run the handle's device work on the caller's stream (a cudaStream_t passed
+ * as void*); NULL restores the handle's own stream.  No counterpart in the
+ * reference, which uses the legacy default stream throughout. */
+pxr_status pxr_set_stream(pxr_handle* h, void* stream);
+
+/* CudaDeviceManager::initialize(const Graph&) (cuda/interface.h:24;
+ * cuda/device.h:86-100).  Uploads the CSR (n+1 offsets, 2m columns), resets
+ * the partition to one cluster and seeds the potentials from cfg.seed.
+ * Offsets are 32-bit (the reference's EdgeIx) or 64-bit. */
+pxr_status pxr_initialize(pxr_handle* h, uint32_t n, uint64_t m,
+                          const uint32_t* offsets, const uint32_t* cols);
+pxr_status pxr_initialize64(pxr_handle* h, uint32_t n, uint64_t m,
+                            const uint64_t* offsets, const uint32_t* cols);
+
+/* CudaDeviceManager::iterateRandomWalk() (cuda/interface.h:29). */
+pxr_status pxr_walk_step(pxr_handle* h);
+/* CudaDeviceManager::computeSweepCuts() (cuda/interface.h:32). */
+pxr_status pxr_sweep(pxr_handle* h);
+/* CudaDeviceManager::cutClusters() (cuda/interface.h:36). */
+pxr_status pxr_cut_clusters(pxr_handle* h);
+/* CudaDeviceManager::expanderDecomposition() (cuda/interface.h:40). *rounds may be NULL. */
+pxr_status pxr_decompose(pxr_handle* h, uint32_t* rounds);
+
+/* CudaDeviceManager::readRandomWalkValues() (cuda/interface.h:30): n floats. */
+pxr_status pxr_read_potentials(pxr_handle* h, float* out);
+/* CudaDeviceManager::readSweepCuts() (cuda/interface.h:34): labels and
+ * per-cluster argmin cuts of every active cluster (before thresholding).
+ * Writes min(cap, count) entries and sets *count. */
+pxr_status pxr_read_sweep_cuts(pxr_handle* h, int32_t* labels, pxr_sweep_cut* cuts,
+                               uint32_t cap, uint32_t* count);
+/* CudaDeviceManager::downloadPartition() (cuda/interface.h:27): the sweep
+ * order with prefix sums, active vertices only.  Writes min(cap, count). */
+pxr_status pxr_download_partition(pxr_handle* h, pxr_node_data* out, uint32_t cap,
+                                  uint32_t* count);
+/* CudaDeviceManager::getFinalPartition() (cuda/interface.h:42): dense ids
+ * 0..k-1 ordered by label value, n entries. */
+pxr_status pxr_final_partition(pxr_handle* h, int32_t* ids, int32_t* num_clusters);
+/* CudaDeviceManager::getNumCutEdges() (cuda/interface.h:38). */
+pxr_status pxr_num_cut_edges(pxr_handle* h, uint64_t* out);
+/* CudaDeviceManager::downloadGraph() (cuda/interface.h:25): the CSR with
+ * disabled slots set to PXR_INVALID_EDGE.  offsets: n+1 entries (32-bit
+ * variant fails with PXR_INVALID_ARG when 2m >= 2^32). */
+pxr_status pxr_download_graph(pxr_handle* h, uint32_t* offsets, uint32_t* cols);
+pxr_status pxr_download_graph64(pxr_handle* h, uint64_t* offsets, uint32_t* cols);
+/* CudaDeviceManager::downloadDegrees() (cuda/interface.h:26): internal degrees. */
+pxr_status pxr_download_degrees(pxr_handle* h, uint32_t* out);
+/* CudaDeviceManager::downloadLabels() (cuda/interface.h:45). */
+pxr_status pxr_download_labels(pxr_handle* h, int32_t* out);
+/* CudaDeviceManager::downloadActiveEdgeMap() (cuda/interface.h:44): 2m ints. */
+pxr_status pxr_active_edge_map(pxr_handle* h, int32_t* out);
+/* CudaDeviceManager::getNumClusters() (cuda/interface.h:46; the reference
+ * returns 0 unconditionally, cuda/device.h:120-123): here the number of
+ * active clusters. */
+pxr_status pxr_num_active_clusters(pxr_handle* h, uint32_t* out);
+
+pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out);
+
+/* Test hooks with no counterpart in the reference: overwrite the potentials
+ * (n doubles, rounded to the product's float storage), or the whole round
+ * state.  act holds the n_act active vertex ids in the order their keys are
+ * emitted; labels of active vertices must be dense in [0, n_clusters). */
+pxr_status pxr_set_potentials(pxr_handle* h, const double* x);
+pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* act, uint32_t n_act,
+                         const double* x, const uint32_t* internal_degrees, const uint32_t* cols,
+                         uint32_t n_clusters, int32_t smallest_label, int full_components);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

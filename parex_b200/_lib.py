@@ -1,0 +1,114 @@
+"""ctypes loader for libparex_b200.so (the C ABI of include/parex_b200.h).
+
+The library is built in-tree by ``parex_b200/build.py``; there is no CPU
+fallback, so a missing or unloadable library raises ImportError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libparex_b200.so")
+
+PXR_OK = 0
+STATUS = {0: "PXR_OK", 1: "PXR_INVALID_ARG", 2: "PXR_OUT_OF_MEMORY", 3: "PXR_ITER_CAP",
+          4: "PXR_CUDA_ERROR", 5: "PXR_DEVICE_FAULT", 6: "PXR_NOT_INITIALIZED"}
+DIV_IEEE = 0
+DIV_REFERENCE = 1
+DRIVER_GRAPH = 0
+DRIVER_STREAM = 1
+
+# every symbol the header declares, in header order
+SYMBOLS = [
+    "pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_create", "pxr_destroy",
+    "pxr_set_stream", "pxr_initialize", "pxr_initialize64", "pxr_walk_step", "pxr_sweep",
+    "pxr_cut_clusters", "pxr_decompose", "pxr_read_potentials", "pxr_read_sweep_cuts",
+    "pxr_download_partition", "pxr_final_partition", "pxr_num_cut_edges", "pxr_download_graph",
+    "pxr_download_graph64", "pxr_download_degrees", "pxr_download_labels", "pxr_active_edge_map",
+    "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_potentials", "pxr_set_state",
+]
+
+
+class Config(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("sc_threshold", C.c_float), ("rw_threshold", C.c_float),
+                ("max_rounds", C.c_uint32), ("device", C.c_int32), ("division", C.c_uint32),
+                ("driver", C.c_uint32), ("reserved", C.c_uint32 * 9)]
+
+
+class SweepCut(C.Structure):
+    _fields_ = [("label", C.c_int32), ("sparsity", C.c_float), ("offset", C.c_uint32)]
+
+
+class NodeData(C.Structure):
+    _fields_ = [("nix", C.c_uint32), ("prefix_volume", C.c_uint32), ("prefix_edge_diff", C.c_int32),
+                ("offset_in_cluster", C.c_uint32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("rounds", C.c_uint32), ("active_vertices", C.c_uint32), ("active_clusters", C.c_uint32),
+                ("clusters_with_cut", C.c_uint32), ("device_bytes", C.c_uint64),
+                ("last_decompose_ms", C.c_double)]
+
+
+class PxrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the library (raises ImportError if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing; build it with parex_b200.build.build()")
+    L = C.CDLL(LIB_PATH)
+    p = C.c_void_p
+    u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
+    L.pxr_config_default.argtypes = [C.POINTER(Config)]
+    L.pxr_config_default.restype = None
+    L.pxr_status_string.argtypes = [C.c_int]
+    L.pxr_status_string.restype = C.c_char_p
+    L.pxr_last_error.argtypes = [p]
+    L.pxr_last_error.restype = C.c_char_p
+    L.pxr_create.argtypes = [C.POINTER(Config), C.POINTER(p)]
+    L.pxr_destroy.argtypes = [p]
+    L.pxr_destroy.restype = None
+    L.pxr_set_stream.argtypes = [p, p]
+    L.pxr_initialize.argtypes = [p, u32, u64, p, p]
+    L.pxr_initialize64.argtypes = [p, u32, u64, p, p]
+    for name in ["pxr_walk_step", "pxr_sweep", "pxr_cut_clusters"]:
+        getattr(L, name).argtypes = [p]
+    L.pxr_decompose.argtypes = [p, C.POINTER(u32)]
+    L.pxr_read_potentials.argtypes = [p, p]
+    L.pxr_read_sweep_cuts.argtypes = [p, p, p, u32, C.POINTER(u32)]
+    L.pxr_download_partition.argtypes = [p, p, u32, C.POINTER(u32)]
+    L.pxr_final_partition.argtypes = [p, p, C.POINTER(i32)]
+    L.pxr_num_cut_edges.argtypes = [p, C.POINTER(u64)]
+    L.pxr_download_graph.argtypes = [p, p, p]
+    L.pxr_download_graph64.argtypes = [p, p, p]
+    L.pxr_download_degrees.argtypes = [p, p]
+    L.pxr_download_labels.argtypes = [p, p]
+    L.pxr_active_edge_map.argtypes = [p, p]
+    L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]
+    L.pxr_get_stats.argtypes = [p, C.POINTER(Stats)]
+    L.pxr_set_potentials.argtypes = [p, p]
+    L.pxr_set_state.argtypes = [p, p, p, u32, p, p, p, u32, i32, C.c_int]
+    for name in SYMBOLS:
+        fn = getattr(L, name)
+        if name not in ("pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_destroy"):
+            fn.restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(handle, status: int) -> None:
+    if status != PXR_OK:
+        L = load()
+        msg = L.pxr_last_error(handle).decode() if handle else L.pxr_status_string(status).decode()
+        raise PxrError(status, msg)

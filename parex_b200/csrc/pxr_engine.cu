@@ -1,0 +1,873 @@
+// Host side of parex_b200: the handle, device memory, the round drivers and
+// the C ABI declared in include/parex_b200.h.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "pxr_kernels.cuh"
+
+using namespace pxr;
+
+namespace pxr {
+constexpr int kSiteFinal = 5;
+constexpr uint32_t kMaxGrid = 148u * 32u;
+
+// ---------------------------------------------------------------------------
+// final partition on the device (PartitionManager::finalizePartition,
+// cuda/devPartition.h:798-823): sort (label, vertex) pairs, rank the distinct
+// labels, scatter the rank back to each vertex.
+
+__global__ void k_fp_keys(const int32_t* lab, uint32_t n, uint32_t* keys, uint32_t* vals) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        keys[i] = (uint32_t)lab[i] ^ 0x80000000u;
+        vals[i] = i;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_fp_rank(const uint32_t* keys0, const uint32_t* keys1,
+                                                    const uint32_t* vals0, const uint32_t* vals1,
+                                                    const uint32_t* sel_ptr, const uint32_t* n_ptr, int32_t* ids,
+                                                    LookbackState lb, const uint32_t* epoch_ptr, RoundCtr* ctr,
+                                                    int32_t* num_out) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = *n_ptr;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(ctr, kSiteFinal);
+    if (tile >= ntiles) return;
+    const uint32_t sel = *sel_ptr;
+    const uint32_t* keys = sel ? keys1 : keys0;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint32_t epoch = *epoch_ptr;
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t heads = 0, run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = first + k;
+        if (i < count && (i == 0 || keys[i] != keys[i - 1])) { heads |= 1u << k; ++run; }
+    }
+    uint64_t total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &total);
+    if (threadIdx.x == 0) {
+        uint64_t ex = 0;
+        if (tile == 0) {
+            lookback_publish(lb, tile, epoch, 2u, total);
+        } else {
+            lookback_publish(lb, tile, epoch, 1u, total);
+            ex = lookback_exclusive<Add64>(lb, tile, epoch, &ctr->err);
+            lookback_publish(lb, tile, epoch, 2u, ex + total);
+        }
+        s_excl = ex;
+        if (tile == ntiles - 1) *num_out = (int32_t)(ex + total);
+    }
+    __syncthreads();
+    uint32_t r = (uint32_t)(s_excl + incl - run);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = first + k;
+        if (i >= count) break;
+        if (heads & (1u << k)) ++r;
+        ids[vals[i]] = (int32_t)r - 1;
+    }
+}
+
+__global__ void k_count_valid(const uint32_t* cols, uint64_t slots, unsigned long long* out) {
+    uint32_t c = 0;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < slots; j += (uint64_t)gridDim.x * blockDim.x)
+        c += cols[j] != kInvalidEdge;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31u) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
+template <typename OffT>
+__global__ void k_degrees(const OffT* off, uint32_t n, uint32_t* ideg, int32_t* lab, uint32_t* act, uint32_t* ids) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        ideg[v] = (uint32_t)(off[v + 1] - off[v]);
+        lab[v] = 0;
+        act[v] = v;
+        ids[v] = v;
+    }
+}
+
+// x~ = x / internal degree for every vertex, and max |x| over every vertex
+__global__ void k_refresh_scaled(const float* x, const uint32_t* ideg, uint32_t n, float* xt, uint32_t* xmax_bits) {
+    uint32_t vmax = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const float xv = x[v];
+        const uint32_t dg = ideg[v];
+        xt[v] = dg ? __double2float_rn(__ddiv_rn((double)xv, (double)dg)) : 0.0f;
+        const uint32_t b = __float_as_uint(fabsf(xv));
+        vmax = b > vmax ? b : vmax;
+    }
+    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+    if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(xmax_bits, vmax);
+}
+
+__global__ void k_bump_site(uint32_t* epoch, RoundCtr* ctr, int site) {
+    epoch[site] += 1;
+    ctr->tile_counter[site] = 0;
+}
+
+inline uint32_t grid_for(uint64_t threads) {
+    const uint64_t g = (threads + kBlock - 1) / kBlock;
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(g, kMaxGrid));
+}
+
+inline uint32_t host_bitlen(uint64_t v) {
+    uint32_t b = 0;
+    while (v) { ++b; v >>= 1; }
+    return b;
+}
+
+}  // namespace pxr
+
+// ---------------------------------------------------------------------------
+
+struct pxr_handle {
+    pxr_config cfg{};
+    std::string err;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    bool initialized = false;
+    bool off64 = false;
+    uint32_t n = 0;
+    uint64_t m = 0, slots = 0;
+    uint32_t maxdeg = 0;
+    uint32_t W = 8;
+    uint32_t nb_bits = 0;
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+
+    void* off = nullptr;
+    uint32_t* cols = nullptr;
+    int32_t* lab = nullptr;
+    uint32_t* ideg = nullptr;
+    float* x = nullptr;
+    float* xt[2] = {nullptr, nullptr};
+    int2* dv = nullptr;
+    uint32_t *parent = nullptr, *acc_max = nullptr, *acc_min = nullptr, *acc_cnt = nullptr;
+    int64_t* acc_sum = nullptr;
+    int32_t* newlab = nullptr;
+    double* avg = nullptr;
+    int32_t* pdif = nullptr;
+    uint32_t* pvol = nullptr;
+    uint32_t* act[2] = {nullptr, nullptr};
+    uint32_t* ids[2] = {nullptr, nullptr};
+    uint64_t* keys[2] = {nullptr, nullptr};
+    uint32_t* vals[2] = {nullptr, nullptr};
+    ClusterTables tab[2]{};
+    uint32_t* cut_off = nullptr;
+    uint8_t* split = nullptr;
+    pxr_sweep_cut* allcuts = nullptr;
+    uint32_t* roots[2] = {nullptr, nullptr};
+    LookbackState lb[6]{};
+    uint32_t* lb_epoch = nullptr;
+    RoundCtr* ctr = nullptr;
+    SortState sort{};
+    uint32_t* sort_end_bit = nullptr;
+    uint32_t* root_end_bit = nullptr;
+    uint32_t* fp_end_bit = nullptr;
+    uint32_t* d_n = nullptr;
+    int32_t* d_num = nullptr;
+    unsigned long long* d_valid = nullptr;
+    RoundCtr* h_ctr = nullptr;  // pinned mirror
+
+    int xcur = 0, tcur = 0, acur = 0;
+    int sweep_tab = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_parity = -1;
+    uint32_t last_rounds = 0;
+    double last_ms = 0.0;
+};
+
+namespace {
+
+pxr_status fail(pxr_handle* h, pxr_status s, const std::string& msg) {
+    if (h) h->err = msg;
+    return s;
+}
+
+pxr_status cuda_fail(pxr_handle* h, cudaError_t e, const char* where) {
+    return fail(h, e == cudaErrorMemoryAllocation ? PXR_OUT_OF_MEMORY : PXR_CUDA_ERROR,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define PXR_CUDA(h, call)                                        \
+    do {                                                         \
+        cudaError_t e_ = (call);                                 \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, #call); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(pxr_handle* h, T** p, size_t count) {
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return e;
+    h->allocs.push_back(q);
+    h->bytes += bytes;
+    *p = static_cast<T*>(q);
+    return cudaSuccess;
+}
+
+void release(pxr_handle* h) {
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    h->graph_parity = -1;
+    for (void* p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    h->bytes = 0;
+    h->initialized = false;
+}
+
+template <typename OffT>
+Dev<OffT> make_dev(pxr_handle* h) {
+    Dev<OffT> d{};
+    d.off = static_cast<const OffT*>(h->off);
+    d.cols = h->cols;
+    d.n = h->n;
+    d.nb_bits = h->nb_bits;
+    d.sc_threshold = h->cfg.sc_threshold;
+    d.rw_threshold = h->cfg.rw_threshold;
+    d.division = h->cfg.division;
+    d.lab = h->lab;
+    d.ideg = h->ideg;
+    d.x = h->x;
+    d.dv = h->dv;
+    d.parent = h->parent;
+    d.acc_max = h->acc_max;
+    d.acc_min = h->acc_min;
+    d.acc_sum = h->acc_sum;
+    d.acc_cnt = h->acc_cnt;
+    d.newlab = h->newlab;
+    d.avg = h->avg;
+    d.pdif = h->pdif;
+    d.pvol = h->pvol;
+    d.cut_off = h->cut_off;
+    d.split = h->split;
+    d.allcuts = h->allcuts;
+    d.roots[0] = h->roots[0];
+    d.roots[1] = h->roots[1];
+    d.lb_scan = h->lb[kSiteScan];
+    d.lb_relabel = h->lb[kSiteRelabel];
+    d.lb_apply = h->lb[kSiteApply];
+    d.lb_ids = h->lb[kSiteIds];
+    d.lb_cvol = h->lb[kSiteCvol];
+    d.lb_epoch = h->lb_epoch;
+    d.ctr = h->ctr;
+    d.sort = h->sort;
+    d.sort_end_bit = h->sort_end_bit;
+    d.root_end_bit = h->root_end_bit;
+    return d;
+}
+
+// ---------------------------------------------------------------------------
+// stages
+
+template <typename OffT, int W>
+cudaError_t op_walk(pxr_handle* h) {
+    Dev<OffT> d = make_dev<OffT>(h);
+    cudaStream_t s = h->stream;
+    k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1);
+    k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
+                                                                      h->xt[h->xcur ^ 1]);
+    k_after_walk<OffT><<<1, 1, 0, s>>>(d);
+    h->xcur ^= 1;
+    return cudaGetLastError();
+}
+
+template <typename OffT, int W>
+cudaError_t op_sweep(pxr_handle* h) {
+    Dev<OffT> d = make_dev<OffT>(h);
+    cudaStream_t s = h->stream;
+    const ClusterTables& t = h->tab[h->tcur];
+    k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0);
+    k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
+    k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+    SortBuffers<uint64_t> b{};
+    b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
+    b.vals[0] = h->vals[0]; b.vals[1] = h->vals[1];
+    b.count = &h->ctr->n_active;
+    b.end_bit = h->sort_end_bit;
+    b.capacity = h->n;
+    cudaError_t e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64);
+    if (e != cudaSuccess) return e;
+    const uint32_t tiles = (h->n + kScanTile - 1) / kScanTile;
+    k_sweep_scan<OffT><<<std::max(tiles, 1u), kBlock, 0, s>>>(d, t, h->keys[0], h->keys[1], h->vals[0], h->vals[1]);
+    k_cluster_cut<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t);
+    h->sweep_tab = h->tcur;
+    return cudaGetLastError();
+}
+
+template <typename OffT, int W>
+cudaError_t op_cut(pxr_handle* h) {
+    Dev<OffT> d = make_dev<OffT>(h);
+    cudaStream_t s = h->stream;
+    const ClusterTables& t = h->tab[h->tcur];
+    const ClusterTables& nt = h->tab[h->tcur ^ 1];
+    const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
+    k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0);
+    k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
+    k_union<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0],
+                                                                       h->keys[1]);
+    k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0],
+                                                                          h->keys[1], h->roots[0]);
+    SortBuffers<uint32_t> rb{};
+    rb.keys[0] = h->roots[0]; rb.keys[1] = h->roots[1];
+    rb.count = &h->ctr->n_roots;
+    rb.end_bit = h->root_end_bit;
+    rb.capacity = h->n;
+    cudaError_t e = radix_sort<uint32_t>(rb, h->sort, &h->ctr->err, s, (int)std::max(1u, host_bitlen(h->n)));
+    if (e != cudaSuccess) return e;
+    k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], h->roots[1], nt);
+    k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1], h->act[h->acur ^ 1]);
+    k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
+    k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt);
+    k_round_end<OffT><<<1, 1, 0, s>>>(d);
+    h->tcur ^= 1;
+    h->acur ^= 1;
+    return cudaGetLastError();
+}
+
+template <typename OffT, int W>
+cudaError_t op_round(pxr_handle* h) {
+    cudaError_t e = op_walk<OffT, W>(h);
+    if (e == cudaSuccess) e = op_sweep<OffT, W>(h);
+    if (e == cudaSuccess) e = op_cut<OffT, W>(h);
+    return e;
+}
+
+enum Op { kOpWalk, kOpSweep, kOpCut, kOpRound };
+
+template <typename OffT>
+cudaError_t dispatch_w(pxr_handle* h, Op op) {
+#define PXR_OPS(WV)                                      \
+    switch (op) {                                        \
+        case kOpWalk: return op_walk<OffT, WV>(h);       \
+        case kOpSweep: return op_sweep<OffT, WV>(h);     \
+        case kOpCut: return op_cut<OffT, WV>(h);         \
+        default: return op_round<OffT, WV>(h);           \
+    }
+    switch (h->W) {
+        case 4: PXR_OPS(4)
+        case 16: PXR_OPS(16)
+        case 32: PXR_OPS(32)
+        default: PXR_OPS(8)
+    }
+#undef PXR_OPS
+}
+
+cudaError_t dispatch(pxr_handle* h, Op op) {
+    return h->off64 ? dispatch_w<uint64_t>(h, op) : dispatch_w<uint32_t>(h, op);
+}
+
+pxr_status check_device_errors(pxr_handle* h) {
+    if (h->h_ctr->err) {
+        const uint32_t e = h->h_ctr->err;
+        h->h_ctr->err = 0;
+        cudaMemsetAsync(&h->ctr->err, 0, sizeof(uint32_t), h->stream);
+        return fail(h, PXR_DEVICE_FAULT, "device-side bounded wait or invariant failed (bits " + std::to_string(e) + ")");
+    }
+    return PXR_OK;
+}
+
+pxr_status sync_ctr(pxr_handle* h) {
+    PXR_CUDA(h, cudaMemcpyAsync(h->h_ctr, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return check_device_errors(h);
+}
+
+pxr_status run_op(pxr_handle* h, Op op) {
+    if (!h) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    cudaError_t e = dispatch(h, op);
+    if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+    return sync_ctr(h);
+}
+
+// ---------------------------------------------------------------------------
+
+pxr_status setup_tables_initial(pxr_handle* h) {
+    // one cluster with every vertex: start 0, size n, volume 2m, root 0
+    std::vector<uint32_t> one = {0u, h->n, (uint32_t)h->slots, 0u, 0u};
+    const ClusterTables& t = h->tab[h->tcur];
+    PXR_CUDA(h, cudaMemcpyAsync(t.start, &one[0], 4, cudaMemcpyHostToDevice, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(t.size, &one[1], 4, cudaMemcpyHostToDevice, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(t.vol, &one[2], 4, cudaMemcpyHostToDevice, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(t.vol_start, &one[3], 4, cudaMemcpyHostToDevice, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(t.root, &one[4], 4, cudaMemcpyHostToDevice, h->stream));
+    PXR_CUDA(h, cudaMemsetAsync(t.best, 0xFF, 8, h->stream));
+    return PXR_OK;
+}
+
+template <typename OffT>
+pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* offsets, const uint32_t* cols) {
+    if (!h) return PXR_INVALID_ARG;
+    if (!offsets || (m > 0 && !cols)) return fail(h, PXR_INVALID_ARG, "null graph pointer");
+    if (n >= 0x7FFFFFFFu) return fail(h, PXR_INVALID_ARG, "n must be below 2^31 - 1");
+    if ((uint64_t)offsets[0] != 0 || (uint64_t)offsets[n] != 2 * m)
+        return fail(h, PXR_INVALID_ARG, "offsets must start at 0 and end at 2m");
+    uint64_t maxdeg = 0;
+    for (uint32_t v = 0; v < n; ++v) {
+        if (offsets[v + 1] < offsets[v]) return fail(h, PXR_INVALID_ARG, "offsets must be non-decreasing");
+        maxdeg = std::max<uint64_t>(maxdeg, (uint64_t)(offsets[v + 1] - offsets[v]));
+    }
+    for (uint64_t j = 0; j < 2 * m; ++j)
+        if (cols[j] >= n) return fail(h, PXR_INVALID_ARG, "column index out of range");
+    PXR_CUDA(h, cudaSetDevice(h->device));
+    release(h);
+    h->n = n;
+    h->m = m;
+    h->slots = 2 * m;
+    h->maxdeg = (uint32_t)maxdeg;
+    h->off64 = sizeof(OffT) == 8;
+    h->nb_bits = host_bitlen(std::max<uint64_t>(n, maxdeg));
+    // lanes per vertex: the power of two nearest the mean degree, 4..32
+    const double mean = n ? (double)(2 * m) / n : 0.0;
+    h->W = mean <= 6.0 ? 4u : mean <= 12.0 ? 8u : mean <= 24.0 ? 16u : 32u;
+    h->xcur = h->tcur = h->acur = 0;
+    const size_t N = std::max<uint32_t>(n, 1);
+    const uint32_t scan_tiles = (uint32_t)((N + kScanTile - 1) / kScanTile) + 1;
+    const uint32_t sort_tiles = (uint32_t)((N + kSortTile - 1) / kSortTile) + 1;
+    cudaError_t e = cudaSuccess;
+#define A(ptr, cnt) if (e == cudaSuccess) e = dalloc(h, ptr, cnt)
+    A(reinterpret_cast<OffT**>(&h->off), (size_t)n + 1);
+    A(&h->cols, std::max<uint64_t>(h->slots, 1));
+    A(&h->lab, N); A(&h->ideg, N); A(&h->x, N); A(&h->xt[0], N); A(&h->xt[1], N);
+    A(&h->dv, N); A(&h->parent, N); A(&h->acc_max, N); A(&h->acc_min, N); A(&h->acc_cnt, N);
+    A(&h->acc_sum, N); A(&h->newlab, N); A(&h->avg, N); A(&h->pdif, N); A(&h->pvol, N);
+    for (int i = 0; i < 2; ++i) {
+        A(&h->act[i], N); A(&h->ids[i], N); A(&h->keys[i], N); A(&h->vals[i], N); A(&h->roots[i], N);
+        A(&h->tab[i].start, N); A(&h->tab[i].size, N); A(&h->tab[i].vol, N); A(&h->tab[i].vol_start, N);
+        A(&h->tab[i].root, N); A(&h->tab[i].best, N);
+    }
+    A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N);
+    for (int i = 0; i < 6; ++i) { A(&h->lb[i].flags, scan_tiles); A(&h->lb[i].agg, scan_tiles); A(&h->lb[i].inc, scan_tiles); }
+    A(&h->lb_epoch, 8); A(&h->ctr, 1);
+    A(&h->sort.hist, kMaxPasses * kRadix); A(&h->sort.bases, kMaxPasses * kRadix);
+    A(&h->sort.pass_info, kMaxPasses + 1); A(&h->sort.tile_ctr, kMaxPasses); A(&h->sort.epoch, 1);
+    A(&h->sort.status, (size_t)sort_tiles * kRadix);
+    A(&h->sort_end_bit, 1); A(&h->root_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
+    A(&h->d_num, 1); A(&h->d_valid, 1);
+#undef A
+    if (e != cudaSuccess) { release(h); return cuda_fail(h, e, "cudaMalloc"); }
+    h->sort.max_tiles = sort_tiles;
+    cudaStream_t s = h->stream;
+    PXR_CUDA(h, cudaMemcpyAsync(h->off, offsets, ((size_t)n + 1) * sizeof(OffT), cudaMemcpyHostToDevice, s));
+    if (m) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, cudaMemcpyHostToDevice, s));
+    for (int i = 0; i < 6; ++i) {
+        PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
+    }
+    PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, 8 * 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->ctr, 0, sizeof(RoundCtr), s));
+    PXR_CUDA(h, cudaMemsetAsync(h->sort.hist, 0, kMaxPasses * kRadix * 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->sort.epoch, 0, 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->sort.status, 0, (size_t)sort_tiles * kRadix * 8, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->sort.pass_info, 0, (kMaxPasses + 1) * 4, s));
+    const uint32_t consts[4] = {host_bitlen(n > 0 ? n - 1 : 0), 32u, n, 0u};
+    PXR_CUDA(h, cudaMemcpyAsync(h->root_end_bit, &consts[0], 4, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(h->fp_end_bit, &consts[1], 4, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(h->d_n, &consts[2], 4, cudaMemcpyHostToDevice, s));
+    if (n) {
+        k_degrees<OffT><<<grid_for(n), kBlock, 0, s>>>(static_cast<const OffT*>(h->off), n, h->ideg, h->lab,
+                                                      h->act[0], h->ids[0]);
+        launch_initial_potentials(h->off, h->off64, n, h->cfg.seed, h->x, &h->ctr->xmax_bits, s);
+        k_refresh_scaled<<<grid_for(n), kBlock, 0, s>>>(h->x, h->ideg, n, h->xt[0], &h->ctr->xmax_bits);
+    }
+    RoundCtr c{};
+    c.n_active = n;
+    c.n_clusters = n ? 1u : 0u;
+    c.smallest = 0;
+    c.full_components = 1;
+    c.done = n ? 0u : 1u;
+    // everything but xmax_bits, which the kernels above produce
+    PXR_CUDA(h, cudaMemcpyAsync(h->ctr, &c, offsetof(RoundCtr, xmax_bits), cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(&h->ctr->full_components, &c.full_components,
+                                sizeof(RoundCtr) - offsetof(RoundCtr, full_components), cudaMemcpyHostToDevice, s));
+    pxr_status st = setup_tables_initial(h);
+    if (st != PXR_OK) return st;
+    PXR_CUDA(h, cudaGetLastError());
+    h->initialized = true;
+    return sync_ctr(h);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+
+extern "C" {
+
+void pxr_config_default(pxr_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->seed = 6582u;
+    cfg->sc_threshold = 0.3f;
+    cfg->rw_threshold = 1e-4f;
+    cfg->max_rounds = 200000u;
+    cfg->device = 0;
+    cfg->division = PXR_DIV_IEEE;
+    cfg->driver = PXR_DRIVER_GRAPH;
+}
+
+const char* pxr_status_string(pxr_status s) {
+    switch (s) {
+        case PXR_OK: return "ok";
+        case PXR_INVALID_ARG: return "invalid argument";
+        case PXR_OUT_OF_MEMORY: return "out of device memory";
+        case PXR_ITER_CAP: return "round cap reached";
+        case PXR_CUDA_ERROR: return "CUDA error";
+        case PXR_DEVICE_FAULT: return "device-side check failed";
+        case PXR_NOT_INITIALIZED: return "not initialized";
+    }
+    return "unknown status";
+}
+
+const char* pxr_last_error(const void* handle) {
+    return handle ? static_cast<const pxr_handle*>(handle)->err.c_str() : "null handle";
+}
+
+pxr_status pxr_create(const pxr_config* cfg, pxr_handle** out) {
+    if (!out) return PXR_INVALID_ARG;
+    *out = nullptr;
+    pxr_handle* h = new (std::nothrow) pxr_handle();
+    if (!h) return PXR_OUT_OF_MEMORY;
+    if (cfg) h->cfg = *cfg; else pxr_config_default(&h->cfg);
+    if (h->cfg.division > PXR_DIV_REFERENCE || h->cfg.driver > PXR_DRIVER_STREAM) {
+        delete h;
+        return PXR_INVALID_ARG;
+    }
+    h->device = h->cfg.device;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) { delete h; return PXR_CUDA_ERROR; }
+    if (h->device < 0 || h->device >= count) { delete h; return PXR_INVALID_ARG; }
+    if (cudaSetDevice(h->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&h->h_ctr, sizeof(RoundCtr)) != cudaSuccess) {
+        delete h;
+        return PXR_CUDA_ERROR;
+    }
+    std::memset(h->h_ctr, 0, sizeof(RoundCtr));
+    h->stream = h->own_stream;
+    static bool attrs_set = false;
+    if (!attrs_set) {
+        radix_sort_prepare<uint64_t>();
+        radix_sort_prepare<uint32_t>();
+        attrs_set = true;
+    }
+    *out = h;
+    return PXR_OK;
+}
+
+void pxr_destroy(pxr_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    release(h);
+    if (h->h_ctr) cudaFreeHost(h->h_ctr);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+}
+
+pxr_status pxr_set_stream(pxr_handle* h, void* stream) {
+    if (!h) return PXR_INVALID_ARG;
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_parity = -1; }
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    return PXR_OK;
+}
+
+pxr_status pxr_initialize(pxr_handle* h, uint32_t n, uint64_t m, const uint32_t* offsets, const uint32_t* cols) {
+    if (2 * m >= (1ull << 32)) return fail(h, PXR_INVALID_ARG, "32-bit offsets need 2m < 2^32");
+    return initialize_impl<uint32_t>(h, n, m, offsets, cols);
+}
+
+pxr_status pxr_initialize64(pxr_handle* h, uint32_t n, uint64_t m, const uint64_t* offsets, const uint32_t* cols) {
+    if (2 * m < (1ull << 32)) {
+        // keep 32-bit offsets on the device when they fit: half the offset traffic
+        std::vector<uint32_t> o32((size_t)n + 1);
+        for (size_t i = 0; i <= n; ++i) o32[i] = (uint32_t)offsets[i];
+        return initialize_impl<uint32_t>(h, n, m, o32.data(), cols);
+    }
+    return initialize_impl<uint64_t>(h, n, m, offsets, cols);
+}
+
+pxr_status pxr_walk_step(pxr_handle* h) { return run_op(h, kOpWalk); }
+pxr_status pxr_sweep(pxr_handle* h) { return run_op(h, kOpSweep); }
+pxr_status pxr_cut_clusters(pxr_handle* h) { return run_op(h, kOpCut); }
+
+pxr_status pxr_decompose(pxr_handle* h, uint32_t* rounds_out) {
+    if (!h) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    cudaEvent_t e0, e1;
+    PXR_CUDA(h, cudaEventCreate(&e0));
+    PXR_CUDA(h, cudaEventCreate(&e1));
+    pxr_status st = sync_ctr(h);
+    const uint32_t start_rounds = h->h_ctr->rounds;
+    PXR_CUDA(h, cudaEventRecord(e0, h->stream));
+    const uint32_t cap = h->cfg.max_rounds;
+    while (st == PXR_OK && !h->h_ctr->done && h->h_ctr->rounds - start_rounds < cap) {
+        cudaError_t e = dispatch(h, kOpRound);
+        if (e != cudaSuccess) { st = cuda_fail(h, e, "round launch"); break; }
+        st = sync_ctr(h);
+    }
+    PXR_CUDA(h, cudaEventRecord(e1, h->stream));
+    PXR_CUDA(h, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->last_ms = ms;
+    h->last_rounds = h->h_ctr->rounds - start_rounds;
+    if (rounds_out) *rounds_out = h->last_rounds;
+    if (st != PXR_OK) return st;
+    if (!h->h_ctr->done) return fail(h, PXR_ITER_CAP, "round cap reached before every cluster was certified");
+    return PXR_OK;
+}
+
+pxr_status pxr_read_potentials(pxr_handle* h, float* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    PXR_CUDA(h, cudaMemcpyAsync(out, h->x, (size_t)h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PXR_OK;
+}
+
+pxr_status pxr_read_sweep_cuts(pxr_handle* h, int32_t* labels, pxr_sweep_cut* cuts, uint32_t cap, uint32_t* count) {
+    if (!h || !count) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    pxr_status st = sync_ctr(h);
+    if (st != PXR_OK) return st;
+    const uint32_t k = h->h_ctr->sweep_k;
+    *count = k;
+    const uint32_t c = std::min(cap, k);
+    if (c && cuts) {
+        PXR_CUDA(h, cudaMemcpyAsync(cuts, h->allcuts, (size_t)c * sizeof(pxr_sweep_cut), cudaMemcpyDeviceToHost, h->stream));
+        PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    if (labels)
+        for (uint32_t i = 0; i < c; ++i) labels[i] = (int32_t)i;
+    return PXR_OK;
+}
+
+pxr_status pxr_download_partition(pxr_handle* h, pxr_node_data* out, uint32_t cap, uint32_t* count) {
+    if (!h || !count) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    pxr_status st = sync_ctr(h);
+    if (st != PXR_OK) return st;
+    const uint32_t na = h->h_ctr->sweep_n;
+    *count = na;
+    const uint32_t c = std::min(cap, na);
+    if (!c || !out) return PXR_OK;
+    const uint32_t sel = h->h_ctr->main_sel;
+    std::vector<uint64_t> keys(c);
+    std::vector<uint32_t> vals(c), pvol(c), starts(h->n ? h->n : 1);
+    std::vector<int32_t> pdif(c);
+    PXR_CUDA(h, cudaMemcpyAsync(keys.data(), h->keys[sel], c * 8ull, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(vals.data(), h->vals[sel], c * 4ull, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(pdif.data(), h->pdif, c * 4ull, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(pvol.data(), h->pvol, c * 4ull, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(starts.data(), h->tab[h->sweep_tab].start, (size_t)h->n * 4, cudaMemcpyDeviceToHost,
+                                h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (uint32_t i = 0; i < c; ++i) {
+        const uint32_t lab = (uint32_t)(keys[i] >> 32);
+        out[i].nix = vals[i];
+        out[i].prefix_volume = pvol[i];
+        out[i].prefix_edge_diff = pdif[i];
+        out[i].offset_in_cluster = i - starts[lab] + 1;
+    }
+    return PXR_OK;
+}
+
+pxr_status pxr_final_partition(pxr_handle* h, int32_t* ids, int32_t* num_clusters) {
+    if (!h || !ids || !num_clusters) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    const uint32_t n = h->n;
+    if (n == 0) { *num_clusters = 0; return PXR_OK; }
+    cudaStream_t s = h->stream;
+    // reuse idle buffers: roots[] as keys, the idle parity of act[] / ids[] as values
+    uint32_t* k0 = h->roots[0];
+    uint32_t* k1 = h->roots[1];
+    uint32_t* v0 = h->act[h->acur ^ 1];
+    uint32_t* v1 = h->ids[h->acur ^ 1];
+    int32_t* out = reinterpret_cast<int32_t*>(h->dv);
+    k_fp_keys<<<grid_for(n), kBlock, 0, s>>>(h->lab, n, k0, v0);
+    SortBuffers<uint32_t> b{};
+    b.keys[0] = k0; b.keys[1] = k1; b.vals[0] = v0; b.vals[1] = v1;
+    b.count = h->d_n;
+    b.end_bit = h->fp_end_bit;
+    b.capacity = n;
+    cudaError_t e = radix_sort<uint32_t>(b, h->sort, &h->ctr->err, s, 32);
+    if (e != cudaSuccess) return cuda_fail(h, e, "final partition sort");
+    k_bump_site<<<1, 1, 0, s>>>(h->lb_epoch, h->ctr, kSiteFinal);
+    const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+    k_fp_rank<<<tiles, kBlock, 0, s>>>(k0, k1, v0, v1, &h->sort.pass_info[kMaxPasses], h->d_n, out, h->lb[kSiteFinal],
+                                       &h->lb_epoch[kSiteFinal], h->ctr, h->d_num);
+    PXR_CUDA(h, cudaGetLastError());
+    PXR_CUDA(h, cudaMemcpyAsync(ids, out, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    PXR_CUDA(h, cudaMemcpyAsync(num_clusters, h->d_num, 4, cudaMemcpyDeviceToHost, s));
+    return sync_ctr(h);
+}
+
+pxr_status pxr_num_cut_edges(pxr_handle* h, uint64_t* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    unsigned long long valid = 0;
+    PXR_CUDA(h, cudaMemsetAsync(h->d_valid, 0, 8, h->stream));
+    if (h->slots) k_count_valid<<<grid_for(h->slots), kBlock, 0, h->stream>>>(h->cols, h->slots, h->d_valid);
+    PXR_CUDA(h, cudaGetLastError());
+    PXR_CUDA(h, cudaMemcpyAsync(&valid, h->d_valid, 8, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    *out = h->m - valid / 2;
+    return PXR_OK;
+}
+
+pxr_status pxr_download_graph64(pxr_handle* h, uint64_t* offsets, uint32_t* cols) {
+    if (!h || !offsets || (h->slots && !cols)) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    if (h->off64) {
+        PXR_CUDA(h, cudaMemcpyAsync(offsets, h->off, ((size_t)h->n + 1) * 8, cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        std::vector<uint32_t> o((size_t)h->n + 1);
+        PXR_CUDA(h, cudaMemcpyAsync(o.data(), h->off, o.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+        PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+        for (size_t i = 0; i < o.size(); ++i) offsets[i] = o[i];
+    }
+    if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(cols, h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PXR_OK;
+}
+
+pxr_status pxr_download_graph(pxr_handle* h, uint32_t* offsets, uint32_t* cols) {
+    if (!h || !offsets) return PXR_INVALID_ARG;
+    if (h->off64) return fail(h, PXR_INVALID_ARG, "graph has 64-bit offsets");
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    PXR_CUDA(h, cudaMemcpyAsync(offsets, h->off, ((size_t)h->n + 1) * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(cols, h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PXR_OK;
+}
+
+pxr_status pxr_download_degrees(pxr_handle* h, uint32_t* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    PXR_CUDA(h, cudaMemcpyAsync(out, h->ideg, (size_t)h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PXR_OK;
+}
+
+pxr_status pxr_download_labels(pxr_handle* h, int32_t* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    PXR_CUDA(h, cudaMemcpyAsync(out, h->lab, (size_t)h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PXR_OK;
+}
+
+pxr_status pxr_active_edge_map(pxr_handle* h, int32_t* out) {
+    if (!h || (h->slots && !out)) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    std::vector<uint32_t> c(h->slots);
+    if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(c.data(), h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (uint64_t j = 0; j < h->slots; ++j) out[j] = c[j] != PXR_INVALID_EDGE ? 1 : 0;
+    return PXR_OK;
+}
+
+pxr_status pxr_num_active_clusters(pxr_handle* h, uint32_t* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    pxr_status st = sync_ctr(h);
+    *out = h->h_ctr->n_clusters;
+    return st;
+}
+
+pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    std::memset(out, 0, sizeof(*out));
+    out->device_bytes = h->bytes;
+    out->rounds = h->last_rounds;
+    out->last_decompose_ms = h->last_ms;
+    if (!h->initialized) return PXR_OK;
+    pxr_status st = sync_ctr(h);
+    out->active_vertices = h->h_ctr->n_active;
+    out->active_clusters = h->h_ctr->n_clusters;
+    out->clusters_with_cut = h->h_ctr->n_cut;
+    return st;
+}
+
+pxr_status pxr_set_potentials(pxr_handle* h, const double* x) {
+    if (!h || !x) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    std::vector<float> xf(h->n);
+    for (uint32_t v = 0; v < h->n; ++v) xf[v] = (float)x[v];
+    PXR_CUDA(h, cudaMemcpyAsync(h->x, xf.data(), (size_t)h->n * 4, cudaMemcpyHostToDevice, h->stream));
+    PXR_CUDA(h, cudaMemsetAsync(&h->ctr->xmax_bits, 0, 4, h->stream));
+    if (h->n)
+        k_refresh_scaled<<<grid_for(h->n), kBlock, 0, h->stream>>>(h->x, h->ideg, h->n, h->xt[h->xcur],
+                                                                    &h->ctr->xmax_bits);
+    PXR_CUDA(h, cudaGetLastError());
+    return sync_ctr(h);
+}
+
+pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* act, uint32_t n_act, const double* x,
+                         const uint32_t* ideg, const uint32_t* cols, uint32_t n_clusters, int32_t smallest,
+                         int full_components) {
+    if (!h || !labels || (n_act && !act) || !x || !ideg || (h->slots && !cols)) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    const uint32_t n = h->n;
+    if (n_act > n) return fail(h, PXR_INVALID_ARG, "n_act exceeds n");
+    std::vector<uint32_t> size(std::max<uint32_t>(n_clusters, 1), 0), vol(std::max<uint32_t>(n_clusters, 1), 0),
+        root(std::max<uint32_t>(n_clusters, 1), 0xFFFFFFFFu);
+    for (uint32_t i = 0; i < n_act; ++i) {
+        const uint32_t v = act[i];
+        if (v >= n) return fail(h, PXR_INVALID_ARG, "active vertex out of range");
+        const int32_t l = labels[v];
+        if (l < 0 || (uint32_t)l >= n_clusters) return fail(h, PXR_INVALID_ARG, "active labels must lie in [0, n_clusters)");
+        size[l] += 1;
+        vol[l] += ideg[v];
+        root[l] = std::min(root[l], v);
+    }
+    std::vector<uint32_t> start(size.size(), 0), vol_start(size.size(), 0);
+    for (uint32_t c = 1; c < n_clusters; ++c) {
+        start[c] = start[c - 1] + size[c - 1];
+        vol_start[c] = vol_start[c - 1] + vol[c - 1];
+    }
+    std::vector<uint32_t> ids(act, act + n_act);
+    std::sort(ids.begin(), ids.end());
+    cudaStream_t s = h->stream;
+    h->tcur = 0;
+    h->acur = 0;
+    const ClusterTables& t = h->tab[0];
+    PXR_CUDA(h, cudaMemcpyAsync(h->lab, labels, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    if (n_act) {
+        PXR_CUDA(h, cudaMemcpyAsync(h->act[0], act, (size_t)n_act * 4, cudaMemcpyHostToDevice, s));
+        PXR_CUDA(h, cudaMemcpyAsync(h->ids[0], ids.data(), (size_t)n_act * 4, cudaMemcpyHostToDevice, s));
+    }
+    PXR_CUDA(h, cudaMemcpyAsync(h->ideg, ideg, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+    if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, cudaMemcpyHostToDevice, s));
+    if (n_clusters) {
+        PXR_CUDA(h, cudaMemcpyAsync(t.start, start.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));
+        PXR_CUDA(h, cudaMemcpyAsync(t.size, size.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));
+        PXR_CUDA(h, cudaMemcpyAsync(t.vol, vol.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));
+        PXR_CUDA(h, cudaMemcpyAsync(t.vol_start, vol_start.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));
+        PXR_CUDA(h, cudaMemcpyAsync(t.root, root.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));
+    }
+    PXR_CUDA(h, cudaStreamSynchronize(s));
+    RoundCtr* c = h->h_ctr;
+    PXR_CUDA(h, cudaMemcpyAsync(c, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, s));
+    PXR_CUDA(h, cudaStreamSynchronize(s));
+    c->n_active = n_act;
+    c->n_clusters = n_clusters;
+    c->smallest = smallest;
+    c->full_components = full_components ? 1u : 0u;
+    c->done = (n_act == 0 || n_clusters == 0) ? 1u : 0u;
+    PXR_CUDA(h, cudaMemcpyAsync(h->ctr, c, sizeof(RoundCtr), cudaMemcpyHostToDevice, s));
+    return pxr_set_potentials(h, x);
+}
+
+}  // extern "C"

@@ -1,0 +1,804 @@
+// Kernels of one decomposition round (sm_100a).  See pxr_round.cuh for the
+// data layout.  Every kernel reads its item counts from RoundCtr, so launches
+// use host-side capacities and a round can be captured in a CUDA graph.
+#pragma once
+
+#include "pxr_round.cuh"
+#include "../../include/parex_b200.h"
+
+namespace pxr {
+
+constexpr int kBlock = 256;
+constexpr int kScanItems = 8;                        // items per thread in look-back kernels
+constexpr int kScanTile = kBlock * kScanItems;
+
+// ---------------------------------------------------------------------------
+// Run aggregation: a thread holds the aggregates of the runs of equal keys in
+// its consecutive items; the interior runs are emitted by the caller, the
+// first and last fragments here.  A warp (or the whole block) whose threads
+// all hold one run of the same key emits a single combined atomic.
+
+template <class Agg>
+__device__ __forceinline__ void emit_fragments(bool has, bool single, uint32_t k_first,
+                                               typename Agg::T a_first, uint32_t k_last,
+                                               typename Agg::T a_last, const Agg& agg) {
+    using T = typename Agg::T;
+    __shared__ uint32_t s_uni[kBlock / 32];
+    __shared__ uint32_t s_key[kBlock / 32];
+    __shared__ T s_agg[kBlock / 32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t k0 = __shfl_sync(0xFFFFFFFFu, k_first, 0);
+    const bool uni = __all_sync(0xFFFFFFFFu, has && single && k_first == k0);
+    T w = uni ? a_first : Agg::identity();
+    if (uni) w = Agg::warp_reduce(w);
+    if (lane == 0) { s_uni[warp] = uni; s_key[warp] = k0; s_agg[warp] = w; }
+    __syncthreads();
+    bool block_uni = true;
+#pragma unroll
+    for (int i = 0; i < kBlock / 32; ++i) block_uni &= s_uni[i] && s_key[i] == s_key[0];
+    if (block_uni) {
+        if (threadIdx.x == 0) {
+            T t = s_agg[0];
+            for (int i = 1; i < kBlock / 32; ++i) t = Agg::combine(t, s_agg[i]);
+            agg.emit(s_key[0], t);
+        }
+    } else if (uni) {
+        if (lane == 0) agg.emit(k0, w);
+    } else if (has) {
+        agg.emit(k_first, a_first);
+        if (!single) agg.emit(k_last, a_last);
+    }
+    __syncthreads();
+}
+
+// argmin of packed (sparsity bits << 32 | ~position): smaller sparsity wins,
+// equal sparsity goes to the later position (the reference's ArgMinOp keeps
+// its right operand on ties, cuda/devSweepCut.h:356-361).
+struct ArgminAgg {
+    using T = unsigned long long;
+    unsigned long long* best;
+    __device__ static T identity() { return ~0ull; }
+    __device__ static T combine(T a, T b) { return a < b ? a : b; }
+    __device__ static T warp_reduce(T v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const T u = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+            v = u < v ? u : v;
+        }
+        return v;
+    }
+    __device__ void emit(uint32_t key, T v) const { atomicMin(&best[key], v); }
+};
+
+struct ClusterAcc {
+    uint32_t mx, mn;
+    int64_t sum;
+    uint32_t cnt;
+};
+
+struct DataAgg {
+    using T = ClusterAcc;
+    uint32_t* acc_max;
+    uint32_t* acc_min;
+    int64_t* acc_sum;
+    uint32_t* acc_cnt;
+    __device__ static T identity() { return {0u, 0xFFFFFFFFu, 0, 0u}; }
+    __device__ static T combine(T a, T b) {
+        return {a.mx > b.mx ? a.mx : b.mx, a.mn < b.mn ? a.mn : b.mn, a.sum + b.sum, a.cnt + b.cnt};
+    }
+    __device__ static T warp_reduce(T v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            T u;
+            u.mx = __shfl_xor_sync(0xFFFFFFFFu, v.mx, o);
+            u.mn = __shfl_xor_sync(0xFFFFFFFFu, v.mn, o);
+            u.sum = __shfl_xor_sync(0xFFFFFFFFu, v.sum, o);
+            u.cnt = __shfl_xor_sync(0xFFFFFFFFu, v.cnt, o);
+            v = combine(v, u);
+        }
+        return v;
+    }
+    __device__ void emit(uint32_t key, T v) const {
+        atomicMax(&acc_max[key], v.mx);
+        atomicMin(&acc_min[key], v.mn);
+        atomic_add_i64(&acc_sum[key], v.sum);
+        atomicAdd(&acc_cnt[key], v.cnt);
+    }
+};
+
+struct CountAgg {
+    using T = uint32_t;
+    uint32_t* dst;
+    __device__ static T identity() { return 0u; }
+    __device__ static T combine(T a, T b) { return a + b; }
+    __device__ static T warp_reduce(T v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        return v;
+    }
+    __device__ void emit(uint32_t key, T v) const { atomicAdd(&dst[key], v); }
+};
+
+// ---------------------------------------------------------------------------
+// dynamic tile id + epoch for a look-back site
+
+__device__ __forceinline__ uint32_t fetch_tile(RoundCtr* ctr, int site) {
+    __shared__ uint32_t s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr->tile_counter[site], 1u);
+    __syncthreads();
+    return s_tile;
+}
+
+__device__ __forceinline__ uint32_t sorted_sel(const SortState& s) { return s.pass_info[kMaxPasses]; }
+
+
+// ---------------------------------------------------------------------------
+// round bookkeeping
+
+template <typename OffT>
+__global__ void k_round_prep(Dev<OffT> d, int walk) {
+    RoundCtr* c = d.ctr;
+    c->n_cut = 0;
+    c->n_roots = 0;
+    if (walk) c->xmax_walk_bits = 0;
+    c->smallest_next = 0;
+    c->n_keep = 0;
+    c->n_active_next = 0;
+    for (int i = 0; i < 8; ++i) {
+        c->tile_counter[i] = 0;
+        d.lb_epoch[i] += 1;
+    }
+    const uint32_t k = c->n_clusters;
+    *d.sort_end_bit = 32u + bitlen(k > 0 ? k - 1 : 0);
+}
+
+template <typename OffT>
+__global__ void k_after_walk(Dev<OffT> d) { d.ctr->xmax_bits = d.ctr->xmax_walk_bits; }
+
+template <typename OffT>
+__global__ void k_round_end(Dev<OffT> d) {
+    RoundCtr* c = d.ctr;
+    if (c->n_active > 0) c->rounds += 1;
+    c->n_active = c->n_active_next;
+    c->n_clusters = c->n_keep;
+    c->smallest = c->smallest_next;
+    c->full_components = 0;
+    c->done = (c->n_active == 0 || c->n_clusters == 0) ? 1u : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// walk: x'[v] = 0.9 * sum_{u ~ v, valid} x[u]/d(u) + 0.1 * x[v]
+// (fusedRandomWalk_WarpParallel, cuda/devRandomWalk.h:117-203), W lanes per
+// vertex, vertices in id order, exact fixed-point sum.
+
+template <typename OffT, int W>
+__global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* ids, const float* xt_in,
+                                                 float* xt_out) {
+    const uint32_t count = d.ctr->n_active;
+    const int e = fixed_exponent(d.ctr->xmax_bits, d.nb_bits);
+    const double scale = pow2(e), inv = pow2(-e);
+    const uint32_t gl = threadIdx.x & (W - 1);
+    const uint32_t groups = (gridDim.x * blockDim.x) / W;
+    const uint32_t warp0 = ((blockIdx.x * blockDim.x + threadIdx.x) & ~31u) / W;
+    uint32_t vmax = 0;
+    for (uint32_t j0 = warp0; j0 < count; j0 += groups) {
+        const uint32_t j = j0 + (threadIdx.x & 31u) / W;
+        const bool valid = j < count;
+        const uint32_t v = valid ? ids[j] : 0u;
+        const OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        int64_t acc = 0;
+        for (OffT s = beg + gl; s < end; s += W) {
+            const uint32_t nb = d.cols[s];
+            if (nb != kInvalidEdge) acc += to_fixed(xt_in[nb], scale);
+        }
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o, W);
+        if (valid && gl == 0) {
+            const double sum = __dmul_rn(__ll2double_rn(acc), inv);
+            const double val = __dadd_rn(__dmul_rn(sum, 0.9), __dmul_rn((double)d.x[v], 0.1));
+            const float xv = __double2float_rn(val);
+            d.x[v] = xv;
+            const uint32_t dg = d.ideg[v];
+            xt_out[v] = dg ? __double2float_rn(__ddiv_rn((double)xv, (double)dg)) : 0.0f;
+            const uint32_t b = __float_as_uint(fabsf(xv));
+            vmax = b > vmax ? b : vmax;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+    if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
+}
+
+// ---------------------------------------------------------------------------
+// edge differences (nodeDiffKernel_Sparse_WarpParallel, cuda/devSweepCut.h:20-112):
+// +1 per valid neighbour after v in (potential, id) order, -1 per neighbour before.
+
+template <typename OffT, int W>
+__global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t* ids) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t gl = threadIdx.x & (W - 1);
+    const uint32_t groups = (gridDim.x * blockDim.x) / W;
+    const uint32_t warp0 = ((blockIdx.x * blockDim.x + threadIdx.x) & ~31u) / W;
+    for (uint32_t j0 = warp0; j0 < count; j0 += groups) {
+        const uint32_t j = j0 + (threadIdx.x & 31u) / W;
+        const bool valid = j < count;
+        const uint32_t v = valid ? ids[j] : 0u;
+        const uint32_t mine = valid ? ordered_bits(d.x[v]) : 0u;
+        const OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        int32_t c = 0;
+        for (OffT s = beg + gl; s < end; s += W) {
+            const uint32_t nb = d.cols[s];
+            if (nb == kInvalidEdge) continue;
+            const uint32_t o = ordered_bits(d.x[nb]);
+            const bool before = o < mine || (o == mine && nb < v);
+            c += before ? -1 : 1;
+        }
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o, W);
+        if (valid && gl == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
+    }
+}
+
+// sort keys in the order of the last sort: (label << 32) | ordered potential
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_emit(Dev<OffT> d, const uint32_t* act, uint64_t* keys,
+                                                 uint32_t* vals, uint64_t* best) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t v = act[i];
+        keys[i] = ((uint64_t)(uint32_t)d.lab[v] << 32) | ordered_bits(d.x[v]);
+        vals[i] = v;
+        if (i < k) best[i] = ~0ull;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sweep scan: inclusive prefix of (edge difference, volume) over the sorted
+// order with a decoupled look-back, then the sparsity of every prefix and the
+// per-cluster argmin (SweepCutTransform + ArgMinOp, cuda/devSweepCut.h:374-433, 665-688).
+
+__device__ __forceinline__ float sweep_ratio(uint32_t num, uint32_t den, uint32_t division) {
+    if (division == PXR_DIV_REFERENCE) return __fdividef((float)num, (float)den);
+    return __fdiv_rn((float)num, (float)den);
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_sweep_scan(Dev<OffT> d, ClusterTables t, const uint64_t* keys0,
+                                                       const uint64_t* keys1, const uint32_t* vals0,
+                                                       const uint32_t* vals1) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteScan);
+    if (tile >= ntiles) return;
+    const uint32_t sel = sorted_sel(d.sort);
+    if (tile == 0 && threadIdx.x == 0) {
+        d.ctr->main_sel = sel;
+        d.ctr->sweep_n = count;
+        d.ctr->sweep_k = d.ctr->n_clusters;
+    }
+    const uint64_t* keys = sel ? keys1 : keys0;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint32_t epoch = d.lb_epoch[kSiteScan];
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+
+    uint32_t lab[kScanItems];
+    uint64_t pre[kScanItems];
+    uint64_t run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = first + k;
+        uint64_t val = 0;
+        lab[k] = 0;
+        if (i < count) {
+            lab[k] = (uint32_t)(keys[i] >> 32);
+            const int2 dv = d.dv[vals[i]];
+            val = ((uint64_t)(uint32_t)dv.y << 32) | (uint32_t)dv.x;
+        }
+        run = PairAdd::combine(run, val);
+        pre[k] = run;
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
+    if (threadIdx.x == 0) {
+        if (tile == 0) {
+            lookback_publish(d.lb_scan, tile, epoch, 2u, tile_total);
+            s_excl = 0;
+        } else {
+            lookback_publish(d.lb_scan, tile, epoch, 1u, tile_total);
+            const uint64_t ex = lookback_exclusive<PairAdd>(d.lb_scan, tile, epoch, &d.ctr->err);
+            lookback_publish(d.lb_scan, tile, epoch, 2u, PairAdd::combine(ex, tile_total));
+            s_excl = ex;
+        }
+    }
+    __syncthreads();
+    // exclusive prefix of this thread = tile exclusive + (block inclusive - own run)
+    const uint32_t lo = (uint32_t)incl - (uint32_t)run;
+    const uint32_t hi = (uint32_t)(incl >> 32) - (uint32_t)(run >> 32);
+    const uint64_t texcl = PairAdd::combine(s_excl, ((uint64_t)hi << 32) | lo);
+
+    bool has = false, single = true;
+    uint32_t k_first = 0, k_last = 0;
+    unsigned long long a_first = ~0ull, a_last = ~0ull;
+    ArgminAgg am{reinterpret_cast<unsigned long long*>(t.best)};
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = first + k;
+        if (i >= count) break;
+        const uint64_t p = PairAdd::combine(texcl, pre[k]);
+        const uint32_t c = lab[k];
+        const int32_t ldif = (int32_t)(uint32_t)p;
+        const uint32_t lvol = (uint32_t)(p >> 32) - t.vol_start[c];
+        const uint32_t tot = t.vol[c];
+        const uint32_t denom = lvol >= tot ? 0u : (lvol < tot - lvol ? lvol : tot - lvol);
+        const float sp = denom > 0 ? sweep_ratio((uint32_t)ldif, denom, d.division) : 2.0f;
+        d.pdif[i] = ldif;
+        d.pvol[i] = lvol;
+        const unsigned long long cand = ((unsigned long long)__float_as_uint(sp) << 32) | (uint32_t)~i;
+        if (!has) {
+            has = true; k_first = c; a_first = cand; k_last = c; a_last = cand;
+        } else if (c == k_last) {
+            a_last = cand < a_last ? cand : a_last;
+            if (single) a_first = a_last;
+        } else {
+            if (!single) am.emit(k_last, a_last);
+            single = false;
+            k_last = c;
+            a_last = cand;
+        }
+    }
+    emit_fragments<ArgminAgg>(has, single, k_first, a_first, k_last, a_last, am);
+}
+
+// per cluster: the best cut, the threshold test (CheckThreshold,
+// cuda/devSweepCut.h:321-331, 701-709) and the components plan.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTables t) {
+    const uint32_t k = d.ctr->n_clusters;
+    const uint32_t full = d.ctr->full_components;
+    pxr_sweep_cut* cuts = reinterpret_cast<pxr_sweep_cut*>(d.allcuts);
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < k; c += gridDim.x * blockDim.x) {
+        const uint64_t b = t.best[c];
+        const uint32_t pos = ~(uint32_t)b;
+        const float sp = __uint_as_float((uint32_t)(b >> 32));
+        const uint32_t off = pos - t.start[c] + 1u;
+        cuts[c].label = (int32_t)c;
+        cuts[c].sparsity = sp;
+        cuts[c].offset = off;
+        const bool cut = sp < d.sc_threshold;
+        d.cut_off[c] = cut ? off : kNoCut;
+        const bool split = cut || full;
+        d.split[c] = split ? 1 : 0;
+        if (cut) atomicAdd(&d.ctr->n_cut, 1u);
+        if (!split) {
+            const uint32_t r = t.root[c];
+            d.acc_max[r] = 0u;
+            d.acc_min[r] = 0xFFFFFFFFu;
+            d.acc_sum[r] = 0;
+            d.acc_cnt[r] = 0u;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// cut (PartitionManager::cutClusters, cuda/devPartition.h:545-622): in a cut
+// cluster, positions past the chosen prefix take a fresh label; every vertex
+// of a split cluster becomes its own union-find root.
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_cut_init(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
+                                                     const uint32_t* vals1, const uint64_t* keys0,
+                                                     const uint64_t* keys1) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
+    const uint32_t sel = d.ctr->main_sel;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint64_t* keys = sel ? keys1 : keys0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(keys[i] >> 32);
+        if (!d.split[c]) continue;
+        const uint32_t v = vals[i];
+        const uint32_t co = d.cut_off[c];
+        const uint32_t pos = i - t.start[c] + 1u;
+        d.lab[v] = (co != kNoCut && pos > co) ? (int32_t)(k + c) : (int32_t)c;
+        d.parent[v] = v;
+        d.acc_max[v] = 0u;
+        d.acc_min[v] = 0xFFFFFFFFu;
+        d.acc_sum[v] = 0;
+        d.acc_cnt[v] = 0u;
+    }
+}
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t v) {
+    uint32_t p = ld_relaxed(&parent[v]);
+    while (p != v) {
+        const uint32_t gp = ld_relaxed(&parent[p]);
+        if (gp != p) {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> r(parent[v]);
+            r.store(gp, cuda::memory_order_relaxed);  // path halving: gp is an ancestor of v
+        }
+        v = p;
+        p = gp;
+    }
+    return v;
+}
+
+// union over same-label valid edges (ConsolidationManager::consolidate,
+// cuda/devConsolidate.h:46-112, 168-204), each undirected edge once.
+template <typename OffT, int W>
+__global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
+                                                  const uint64_t* keys0, const uint64_t* keys1) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t sel = d.ctr->main_sel;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint64_t* keys = sel ? keys1 : keys0;
+    const uint32_t gl = threadIdx.x & (W - 1);
+    const uint32_t groups = (gridDim.x * blockDim.x) / W;
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) / W; j < count; j += groups) {
+        const uint32_t c = (uint32_t)(keys[j] >> 32);
+        if (!d.split[c]) continue;
+        const uint32_t v = vals[j];
+        const int32_t lv = d.lab[v];
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        for (OffT s = beg + gl; s < end; s += W) {
+            const uint32_t nb = d.cols[s];
+            if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
+            uint32_t a = v, b = nb;
+            for (uint32_t tries = 0;; ++tries) {
+                if (tries > kSpinLimit) { atomicOr(&d.ctr->err, kErrUnionFind); break; }
+                const uint32_t ra = uf_find(d.parent, a), rb = uf_find(d.parent, b);
+                if (ra == rb) break;
+                const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+                if (atomicCAS(&d.parent[hi], hi, lo) == hi) break;
+                a = hi;
+                b = lo;
+            }
+        }
+    }
+}
+
+// roots, per-cluster data (computeClusterData, cuda/devPartition.h:380-411)
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
+                                                            const uint32_t* vals1, const uint64_t* keys0,
+                                                            const uint64_t* keys1, uint32_t* roots) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t sel = d.ctr->main_sel;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint64_t* keys = sel ? keys1 : keys0;
+    const int e = fixed_exponent(d.ctr->xmax_walk_bits, d.nb_bits);
+    const double scale = pow2(e);
+    DataAgg agg{d.acc_max, d.acc_min, d.acc_sum, d.acc_cnt};
+    const uint32_t stride = gridDim.x * kScanTile;
+    for (uint32_t base = blockIdx.x * kScanTile; base < count; base += stride) {
+        const uint32_t first = base + threadIdx.x * kScanItems;
+        bool has = false, single = true;
+        uint32_t k_first = 0, k_last = 0;
+        ClusterAcc a_first = DataAgg::identity(), a_last = DataAgg::identity();
+        for (int k = 0; k < kScanItems; ++k) {
+            const uint32_t i = first + k;
+            if (i >= count) break;
+            const uint32_t c = (uint32_t)(keys[i] >> 32);
+            const uint32_t v = vals[i];
+            uint32_t r;
+            if (d.split[c]) {
+                r = uf_find(d.parent, v);
+                cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(d.parent[v]).store(r, cuda::memory_order_relaxed);
+                if (r == v) roots[atomicAdd(&d.ctr->n_roots, 1u)] = r;
+            } else {
+                r = t.root[c];
+                if (i == t.start[c]) roots[atomicAdd(&d.ctr->n_roots, 1u)] = r;
+            }
+            const float xv = d.x[v];
+            const uint32_t ob = ordered_bits(xv);
+            const ClusterAcc cur{ob, ob, to_fixed(xv, scale), 1u};
+            if (!has) {
+                has = true; k_first = r; a_first = cur; k_last = r; a_last = cur;
+            } else if (r == k_last) {
+                a_last = DataAgg::combine(a_last, cur);
+                if (single) a_first = a_last;
+            } else {
+                if (!single) agg.emit(k_last, a_last);
+                single = false;
+                k_last = r;
+                a_last = cur;
+            }
+        }
+        emit_fragments<DataAgg>(has, single, k_first, a_first, k_last, a_last, agg);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// keep / deactivate and dense relabel (recenterAndDeactivateClusters,
+// cuda/devPartition.h:624-711): roots sorted by vertex id; kept clusters get
+// dense labels in root order, dropped ones smallest - index - 1.
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t* roots0, const uint32_t* roots1,
+                                                    ClusterTables nt) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = d.ctr->n_roots;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteRelabel);
+    if (tile >= ntiles) return;
+    const uint32_t sel = sorted_sel(d.sort);
+    const uint32_t* roots = sel ? roots1 : roots0;
+    const uint32_t epoch = d.lb_epoch[kSiteRelabel];
+    const int e = fixed_exponent(d.ctr->xmax_walk_bits, d.nb_bits);
+    const double inv = pow2(-e);
+    const int32_t smallest = d.ctr->smallest;
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint64_t vals[kScanItems];
+    uint64_t run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t j = first + k;
+        uint64_t v = 0;
+        if (j < count) {
+            const uint32_t r = roots[j];
+            const uint32_t cnt = d.acc_cnt[r];
+            const float pot = __fsub_rn(from_ordered_bits(d.acc_max[r]), from_ordered_bits(d.acc_min[r]));
+            const bool keep = pot >= d.rw_threshold && cnt >= 2;
+            v = keep ? (((uint64_t)cnt << 32) | 1u) : 0ull;
+        }
+        vals[k] = v;
+        run = PairAdd::combine(run, v);
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
+    if (threadIdx.x == 0) {
+        uint64_t ex = 0;
+        if (tile == 0) {
+            lookback_publish(d.lb_relabel, tile, epoch, 2u, tile_total);
+        } else {
+            lookback_publish(d.lb_relabel, tile, epoch, 1u, tile_total);
+            ex = lookback_exclusive<PairAdd>(d.lb_relabel, tile, epoch, &d.ctr->err);
+            lookback_publish(d.lb_relabel, tile, epoch, 2u, PairAdd::combine(ex, tile_total));
+        }
+        s_excl = ex;
+        if (tile == ntiles - 1) {
+            const uint64_t all = PairAdd::combine(ex, tile_total);
+            d.ctr->n_keep = (uint32_t)all;
+            d.ctr->n_active_next = (uint32_t)(all >> 32);
+        }
+    }
+    __syncthreads();
+    const uint32_t lo = (uint32_t)incl - (uint32_t)run;
+    const uint32_t hi = (uint32_t)(incl >> 32) - (uint32_t)(run >> 32);
+    uint64_t p = PairAdd::combine(s_excl, ((uint64_t)hi << 32) | lo);
+    int32_t most_negative = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t j = first + k;
+        if (j >= count) break;
+        const uint32_t r = roots[j];
+        if (vals[k]) {
+            const uint32_t nl = (uint32_t)p;
+            const uint32_t cnt = (uint32_t)(vals[k] >> 32);
+            d.newlab[r] = (int32_t)nl;
+            d.avg[r] = __ddiv_rn(__dmul_rn(__ll2double_rn(d.acc_sum[r]), inv), (double)cnt);
+            nt.size[nl] = cnt;
+            nt.start[nl] = (uint32_t)(p >> 32);
+            nt.root[nl] = r;
+            nt.best[nl] = ~0ull;
+            nt.vol[nl] = 0u;
+        } else {
+            const int32_t nl = (int32_t)((uint32_t)smallest - j - 1u);
+            d.newlab[r] = nl;
+            most_negative = nl < most_negative ? nl : most_negative;
+        }
+        p = PairAdd::combine(p, vals[k]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) most_negative = min(most_negative, __shfl_xor_sync(0xFFFFFFFFu, most_negative, o));
+    if ((threadIdx.x & 31u) == 0 && most_negative < 0) atomicMin(&d.ctr->smallest_next, most_negative);
+}
+
+// new labels, recentering (x -= cluster mean) and the stable compaction of
+// the sorted order into the next round's active list.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
+                                                  const uint32_t* vals1, const uint64_t* keys0,
+                                                  const uint64_t* keys1, uint32_t* act_next) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteApply);
+    if (tile == 0 && threadIdx.x == 0) d.ctr->xmax_bits = 0;
+    if (tile >= ntiles) return;
+    const uint32_t sel = d.ctr->main_sel;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint64_t* keys = sel ? keys1 : keys0;
+    const uint32_t epoch = d.lb_epoch[kSiteApply];
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t vv[kScanItems];
+    uint32_t keepmask = 0, run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = first + k;
+        vv[k] = 0;
+        if (i >= count) continue;
+        const uint32_t c = (uint32_t)(keys[i] >> 32);
+        const uint32_t v = vals[i];
+        vv[k] = v;
+        // find() again: a concurrent path-halving step in k_components_data may
+        // have replaced the stored root of v by a (non-root) ancestor
+        const uint32_t r = d.split[c] ? uf_find(d.parent, v) : t.root[c];
+        const int32_t nl = d.newlab[r];
+        d.lab[v] = nl;
+        if (nl >= 0) {
+            d.x[v] = __double2float_rn(__dsub_rn((double)d.x[v], d.avg[r]));
+            keepmask |= 1u << k;
+            ++run;
+        }
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &tile_total);
+    if (threadIdx.x == 0) {
+        uint64_t ex = 0;
+        if (tile == 0) {
+            lookback_publish(d.lb_apply, tile, epoch, 2u, tile_total);
+        } else {
+            lookback_publish(d.lb_apply, tile, epoch, 1u, tile_total);
+            ex = lookback_exclusive<Add64>(d.lb_apply, tile, epoch, &d.ctr->err);
+            lookback_publish(d.lb_apply, tile, epoch, 2u, ex + tile_total);
+        }
+        s_excl = ex;
+    }
+    __syncthreads();
+    uint32_t pos = (uint32_t)(s_excl + incl - run);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (keepmask & (1u << k)) act_next[pos++] = vv[k];
+}
+
+// next round's vertex-order list, edge disabling (disableEdgesKernel_node,
+// cuda/devPartition.h:80-146), internal degrees, x/d, cluster volumes.
+template <typename OffT, int W>
+__global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint32_t* ids, uint32_t* ids_next,
+                                                        float* xt, ClusterTables nt) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    __shared__ uint32_t s_list[kScanTile];
+    __shared__ uint32_t s_hkey[kScanTile];
+    __shared__ uint32_t s_hval[kScanTile];
+    __shared__ uint32_t s_n;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteIds);
+    if (tile >= ntiles) return;
+    const uint32_t epoch = d.lb_epoch[kSiteIds];
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t vv[kScanItems];
+    uint32_t keepmask = 0, run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t j = first + k;
+        vv[k] = 0;
+        if (j >= count) continue;
+        const uint32_t v = ids[j];
+        vv[k] = v;
+        if (d.lab[v] >= 0) { keepmask |= 1u << k; ++run; }
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &tile_total);
+    if (threadIdx.x == 0) {
+        uint64_t ex = 0;
+        if (tile == 0) {
+            lookback_publish(d.lb_ids, tile, epoch, 2u, tile_total);
+        } else {
+            lookback_publish(d.lb_ids, tile, epoch, 1u, tile_total);
+            ex = lookback_exclusive<Add64>(d.lb_ids, tile, epoch, &d.ctr->err);
+            lookback_publish(d.lb_ids, tile, epoch, 2u, ex + tile_total);
+        }
+        s_excl = ex;
+        s_n = (uint32_t)tile_total;
+    }
+    __syncthreads();
+    uint32_t lpos = (uint32_t)(incl - run);
+    const uint32_t gpos = (uint32_t)s_excl;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (keepmask & (1u << k)) {
+            ids_next[gpos + lpos] = vv[k];
+            s_list[lpos] = vv[k];
+            ++lpos;
+        }
+    __syncthreads();
+    // row pass over this tile's kept vertices, W lanes per vertex; cluster
+    // volumes are summed per tile in a shared hash table keyed by label
+    for (uint32_t q = threadIdx.x; q < kScanTile; q += kBlock) { s_hkey[q] = 0xFFFFFFFFu; s_hval[q] = 0u; }
+    __syncthreads();
+    const uint32_t nkept = s_n;
+    const uint32_t gl = threadIdx.x & (W - 1);
+    uint32_t vmax = 0;
+    for (uint32_t q0 = (threadIdx.x & ~31u) / W; q0 < nkept; q0 += kBlock / W) {
+        const uint32_t q = q0 + (threadIdx.x & 31u) / W;
+        const bool valid = q < nkept;
+        const uint32_t v = valid ? s_list[q] : 0u;
+        const int32_t lv = valid ? d.lab[v] : 0;
+        const OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        uint32_t deg = 0;
+        for (OffT s = beg + gl; s < end; s += W) {
+            const uint32_t nb = d.cols[s];
+            if (nb == kInvalidEdge) continue;
+            if (d.lab[nb] != lv) d.cols[s] = kInvalidEdge;
+            else ++deg;
+        }
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) deg += __shfl_xor_sync(0xFFFFFFFFu, deg, o, W);
+        if (valid && gl == 0) {
+            d.ideg[v] = deg;
+            const float xv = d.x[v];
+            xt[v] = deg ? __double2float_rn(__ddiv_rn((double)xv, (double)deg)) : 0.0f;
+            const uint32_t b = __float_as_uint(fabsf(xv));
+            vmax = b > vmax ? b : vmax;
+            uint32_t h = ((uint32_t)lv * 2654435761u) & (kScanTile - 1);
+            for (;;) {
+                const uint32_t prev = atomicCAS(&s_hkey[h], 0xFFFFFFFFu, (uint32_t)lv);
+                if (prev == 0xFFFFFFFFu || prev == (uint32_t)lv) { atomicAdd(&s_hval[h], deg); break; }
+                h = (h + 1) & (kScanTile - 1);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+    if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(&d.ctr->xmax_bits, vmax);
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < kScanTile; q += kBlock)
+        if (s_hkey[q] != 0xFFFFFFFFu && s_hval[q]) atomicAdd(&nt.vol[s_hkey[q]], s_hval[q]);
+}
+
+// exclusive prefix of cluster volumes over labels
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_cvol_scan(Dev<OffT> d, ClusterTables nt) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = d.ctr->n_keep;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteCvol);
+    if (tile >= ntiles) return;
+    const uint32_t epoch = d.lb_epoch[kSiteCvol];
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint64_t run = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t j = first + k;
+        v[k] = j < count ? nt.vol[j] : 0u;
+        run += v[k];
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<Add64>(run, warp_tot, &tile_total);
+    if (threadIdx.x == 0) {
+        uint64_t ex = 0;
+        if (tile == 0) {
+            lookback_publish(d.lb_cvol, tile, epoch, 2u, tile_total);
+        } else {
+            lookback_publish(d.lb_cvol, tile, epoch, 1u, tile_total);
+            ex = lookback_exclusive<Add64>(d.lb_cvol, tile, epoch, &d.ctr->err);
+            lookback_publish(d.lb_cvol, tile, epoch, 2u, ex + tile_total);
+        }
+        s_excl = ex;
+    }
+    __syncthreads();
+    uint64_t p = s_excl + incl - run;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t j = first + k;
+        if (j >= count) break;
+        nt.vol_start[j] = (uint32_t)p;
+        p += v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// initial potentials (RandomWalkManager::initRandomWalk, cuda/devRandomWalk.h:22-48, 509-519)
+void launch_initial_potentials(const void* off, bool off64, uint32_t n, uint32_t seed, float* x,
+                               uint32_t* xmax_bits, cudaStream_t stream);
+
+}  // namespace pxr

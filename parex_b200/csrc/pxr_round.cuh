@@ -1,0 +1,83 @@
+// Device state and kernels of one decomposition round (sm_100a).
+//
+// The round follows the reference's stage order (cuda/device.h:101-168,
+// 363-404): walk step, sweep (edge differences, stable sort by
+// (cluster, potential), prefix scan, sparsest prefix per cluster), cut,
+// connected components, per-cluster reductions, deactivation and recentering,
+// edge disabling.  Layout and arithmetic are this project's own:
+//
+//  * potentials are float; the walk and the per-cluster sums accumulate
+//    exactly in int64 fixed point (scale 2^e chosen from the largest |x| and
+//    the largest term count), so results do not depend on the order in which
+//    threads add terms;
+//  * per-cluster tables (start, size, volume, start volume, root vertex) are
+//    produced at the end of a round, so the next sweep is a single
+//    unsegmented look-back scan: the edge differences of a cluster sum to
+//    zero and its start volume is known;
+//  * components use lock-free union-find (hook the larger root under the
+//    smaller with atomicCAS, path halving), which labels every component by
+//    its minimum vertex id, the reference's canonical root;
+//  * active vertices are kept twice: `act` in the order of the last sort (the
+//    stable sort's tie order) and `ids` in vertex order (coalesced row work).
+#pragma once
+
+#include "pxr_common.cuh"
+#include "pxr_sort.cuh"
+
+namespace pxr {
+
+struct ClusterTables {
+    uint32_t* start;      // first sorted position of the cluster
+    uint32_t* size;       // vertices
+    uint32_t* vol;        // internal volume (sum of internal degrees)
+    uint32_t* vol_start;  // exclusive prefix of vol over labels
+    uint32_t* root;       // minimum vertex id
+    uint64_t* best;       // packed (sparsity bits, ~position) argmin
+};
+
+template <typename OffT>
+struct Dev {
+    // graph
+    const OffT* off;
+    uint32_t* cols;
+    uint32_t n;
+    uint32_t nb_bits;     // bit length of max(n, max row length)
+    float sc_threshold;
+    float rw_threshold;
+    uint32_t division;    // PXR_DIV_*
+    // per vertex
+    int32_t* lab;
+    uint32_t* ideg;
+    float* x;
+    int2* dv;             // {edge difference, internal degree}
+    uint32_t* parent;
+    uint32_t* acc_max;    // ordered float bits, by root vertex
+    uint32_t* acc_min;
+    int64_t* acc_sum;
+    uint32_t* acc_cnt;
+    int32_t* newlab;      // by root vertex
+    double* avg;          // by root vertex
+    // per sorted position
+    int32_t* pdif;
+    uint32_t* pvol;
+    // per cluster
+    uint32_t* cut_off;
+    uint8_t* split;
+    void* allcuts;        // pxr_sweep_cut[]
+    // roots after the components stage
+    uint32_t* roots[2];
+    // look-back state
+    LookbackState lb_scan, lb_relabel, lb_apply, lb_ids, lb_cvol;
+    uint32_t* lb_epoch;   // [8] current epoch per look-back site
+    RoundCtr* ctr;
+    SortState sort;
+    uint32_t* sort_end_bit;   // main sort bits
+    uint32_t* root_end_bit;   // root sort bits
+};
+
+// look-back sites (index into Dev::lb_epoch and RoundCtr::tile_counter)
+enum : int { kSiteScan = 0, kSiteRelabel = 1, kSiteApply = 2, kSiteIds = 3, kSiteCvol = 4 };
+
+__device__ __forceinline__ uint32_t bitlen(uint32_t v) { return v ? 32u - __clz(v) : 0u; }
+
+}  // namespace pxr

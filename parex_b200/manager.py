@@ -1,0 +1,207 @@
+"""Python mirror of the reference's drop-in class CudaDeviceManager (cuda/interface.h:16-57).
+
+Method names, argument meaning and return values follow the reference:
+
+=========================  =====================================================
+reference member            here
+=========================  =====================================================
+initialize(const Graph&)    initialize(graph)  (a CSRGraph or (offsets, cols))
+downloadGraph()             downloadGraph() -> (offsets, cols), disabled = 0xFFFFFFFF
+downloadDegrees()           downloadDegrees() -> internal degrees (uint32[n])
+downloadPartition()         downloadPartition() -> NodeData records in sweep order
+iterateRandomWalk()         iterateRandomWalk()
+readRandomWalkValues()      readRandomWalkValues() -> float32[n]
+computeSweepCuts()          computeSweepCuts()
+readSweepCuts()             readSweepCuts() -> AllSweepCuts(clusterIds, cuts)
+cutClusters()               cutClusters()
+getNumCutEdges()            getNumCutEdges()
+expanderDecomposition()     expanderDecomposition() -> rounds run
+getFinalPartition()         getFinalPartition() -> FinalPartition(clusterIds, numClusters)
+downloadActiveEdgeMap()     downloadActiveEdgeMap() -> int32[2m]
+downloadLabels()            downloadLabels() -> int32[n]
+getNumClusters()            getNumClusters() (the reference returns 0; here the
+                            number of active clusters)
+updateLabels(...)           updateLabels(...) (a no-op, as in cuda/devGraph.h:191-206)
+=========================  =====================================================
+
+Errors raise ``PxrError`` carrying the C status; the reference has no error
+reporting at all.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import NamedTuple
+
+import numpy as np
+
+from . import _lib
+from .graphs import CSRGraph
+
+NODE_DATA = np.dtype([("nix", "<u4"), ("prefix_volume", "<u4"), ("prefix_edge_diff", "<i4"),
+                      ("offset_in_cluster", "<u4")])
+SWEEP_CUT = np.dtype([("label", "<i4"), ("sparsity", "<f4"), ("offset", "<u4")])
+
+
+class AllSweepCuts(NamedTuple):
+    clusterIds: np.ndarray
+    cuts: np.ndarray
+
+
+class FinalPartition(NamedTuple):
+    clusterIds: np.ndarray
+    numClusters: int
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class CudaDeviceManager:
+    """One decomposition on one GPU; not thread-safe (like the reference)."""
+
+    def __init__(self, seed: int = 6582, sc_threshold: float = 0.3, rw_threshold: float = 1e-4,
+                 max_rounds: int = 200000, device: int = 0, division: int = _lib.DIV_IEEE,
+                 driver: int = _lib.DRIVER_GRAPH):
+        L = _lib.load()
+        cfg = _lib.Config()
+        L.pxr_config_default(C.byref(cfg))
+        cfg.seed = seed
+        cfg.sc_threshold = sc_threshold
+        cfg.rw_threshold = rw_threshold
+        cfg.max_rounds = max_rounds
+        cfg.device = device
+        cfg.division = division
+        cfg.driver = driver
+        self._h = C.c_void_p()
+        _lib.check(None, L.pxr_create(C.byref(cfg), C.byref(self._h)))
+        self._L = L
+        self.n = 0
+        self.m = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.pxr_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, fn, *args):
+        _lib.check(self._h, fn(self._h, *args))
+
+    # -- reference members ------------------------------------------------
+    def initialize(self, graph) -> None:
+        if isinstance(graph, CSRGraph):
+            offsets, cols = graph.offsets, graph.cols
+        else:
+            offsets, cols = graph
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        n = int(offsets.shape[0] - 1)
+        m = int(cols.shape[0] // 2)
+        if offsets.dtype == np.uint64 or 2 * m >= 2**32:
+            off = np.ascontiguousarray(offsets, dtype=np.uint64)
+            self._call(self._L.pxr_initialize64, n, m, _ptr(off), _ptr(cols))
+        else:
+            off = np.ascontiguousarray(offsets, dtype=np.uint32)
+            self._call(self._L.pxr_initialize, n, m, _ptr(off), _ptr(cols))
+        self.n, self.m = n, m
+
+    def iterateRandomWalk(self) -> None:
+        self._call(self._L.pxr_walk_step)
+
+    def computeSweepCuts(self) -> None:
+        self._call(self._L.pxr_sweep)
+
+    def cutClusters(self) -> None:
+        self._call(self._L.pxr_cut_clusters)
+
+    def expanderDecomposition(self) -> int:
+        rounds = C.c_uint32(0)
+        self._call(self._L.pxr_decompose, C.byref(rounds))
+        return int(rounds.value)
+
+    def readRandomWalkValues(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.float32)
+        self._call(self._L.pxr_read_potentials, _ptr(out))
+        return out
+
+    def readSweepCuts(self) -> AllSweepCuts:
+        count = C.c_uint32(0)
+        self._call(self._L.pxr_read_sweep_cuts, None, None, 0, C.byref(count))
+        k = int(count.value)
+        labels = np.zeros(k, dtype=np.int32)
+        cuts = np.zeros(k, dtype=SWEEP_CUT)
+        self._call(self._L.pxr_read_sweep_cuts, _ptr(labels), _ptr(cuts), k, C.byref(count))
+        return AllSweepCuts(labels, cuts)
+
+    def downloadPartition(self) -> np.ndarray:
+        count = C.c_uint32(0)
+        self._call(self._L.pxr_download_partition, None, 0, C.byref(count))
+        out = np.zeros(int(count.value), dtype=NODE_DATA)
+        self._call(self._L.pxr_download_partition, _ptr(out), out.shape[0], C.byref(count))
+        return out
+
+    def getFinalPartition(self) -> FinalPartition:
+        ids = np.zeros(self.n, dtype=np.int32)
+        k = C.c_int32(0)
+        self._call(self._L.pxr_final_partition, _ptr(ids), C.byref(k))
+        return FinalPartition(ids, int(k.value))
+
+    def getNumCutEdges(self) -> int:
+        out = C.c_uint64(0)
+        self._call(self._L.pxr_num_cut_edges, C.byref(out))
+        return int(out.value)
+
+    def downloadGraph(self):
+        offsets = np.zeros(self.n + 1, dtype=np.uint64)
+        cols = np.zeros(2 * self.m, dtype=np.uint32)
+        self._call(self._L.pxr_download_graph64, _ptr(offsets), _ptr(cols))
+        return offsets, cols
+
+    def downloadDegrees(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.uint32)
+        self._call(self._L.pxr_download_degrees, _ptr(out))
+        return out
+
+    def downloadLabels(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.int32)
+        self._call(self._L.pxr_download_labels, _ptr(out))
+        return out
+
+    def downloadActiveEdgeMap(self) -> np.ndarray:
+        out = np.zeros(2 * self.m, dtype=np.int32)
+        self._call(self._L.pxr_active_edge_map, _ptr(out))
+        return out
+
+    def getNumClusters(self) -> int:
+        out = C.c_uint32(0)
+        self._call(self._L.pxr_num_active_clusters, C.byref(out))
+        return int(out.value)
+
+    def updateLabels(self, nodeLabels=None, activeClusters=None) -> None:
+        """No-op, as GraphManager::updateLabels is in the reference."""
+
+    # -- extras -----------------------------------------------------------
+    def stats(self) -> dict:
+        st = _lib.Stats()
+        self._call(self._L.pxr_get_stats, C.byref(st))
+        return {f: getattr(st, f) for f, _ in _lib.Stats._fields_}
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._call(self._L.pxr_set_stream, C.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def set_potentials(self, x) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        self._call(self._L.pxr_set_potentials, _ptr(x))
+
+    def set_state(self, labels, act, x, ideg, cols, n_clusters, smallest, full_components=True) -> None:
+        labels = np.ascontiguousarray(labels, dtype=np.int32)
+        act = np.ascontiguousarray(act, dtype=np.uint32)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        ideg = np.ascontiguousarray(ideg, dtype=np.uint32)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        self._call(self._L.pxr_set_state, _ptr(labels), _ptr(act), act.shape[0], _ptr(x), _ptr(ideg),
+                   _ptr(cols), int(n_clusters), int(smallest), 1 if full_components else 0)
