@@ -76,7 +76,20 @@ typedef struct {
     uint32_t clusters_with_cut;  /* numClustersWithCut of the last sweep                  */
     uint64_t device_bytes;       /* device memory held by the handle                      */
     double last_decompose_ms;    /* device time of the last pxr_decompose (CUDA events)    */
+    uint64_t kernel_launches;    /* kernels this handle has launched since creation        */
+    uint64_t walk_vertices;      /* vertex updates done by walk steps since initialization */
+    uint64_t walk_slots;         /* CSR slots read by walk steps since initialization      */
+    uint64_t walk_gathers;       /* valid-neighbour gathers by walk steps                  */
+    uint64_t sort_items;         /* items x passes moved by the sweep sort                 */
 } pxr_stats;
+
+/* Per-phase device time, recorded with CUDA events when profiling is on
+ * (pxr_set_profiling) and the stream driver runs the rounds. */
+typedef struct {
+    char name[24];
+    double ms;                   /* summed device time                                    */
+    uint64_t launches;           /* kernel launches in this phase                         */
+} pxr_phase_stat;
 
 void pxr_config_default(pxr_config* cfg);
 const char* pxr_status_string(pxr_status s);
@@ -102,6 +115,13 @@ pxr_status pxr_initialize(pxr_handle* h, uint32_t n, uint64_t m,
                           const uint32_t* offsets, const uint32_t* cols);
 pxr_status pxr_initialize64(pxr_handle* h, uint32_t n, uint64_t m,
                             const uint64_t* offsets, const uint32_t* cols);
+/* The same with the CSR already in device memory (device pointers on the
+ * handle's device; offsets 64-bit when offsets_are_64bit, else 32-bit).  The
+ * arrays are copied; the caller keeps ownership.  Repeated initialisation
+ * with the same n and m reuses the handle's device memory. */
+pxr_status pxr_initialize_device(pxr_handle* h, uint32_t n, uint64_t m,
+                                 const void* offsets, int offsets_are_64bit,
+                                 const uint32_t* cols);
 
 /* CudaDeviceManager::iterateRandomWalk() (cuda/interface.h:29). */
 pxr_status pxr_walk_step(pxr_handle* h);
@@ -145,6 +165,11 @@ pxr_status pxr_active_edge_map(pxr_handle* h, int32_t* out);
 pxr_status pxr_num_active_clusters(pxr_handle* h, uint32_t* out);
 
 pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out);
+/* Turn per-phase CUDA-event timing on (1) or off (0); it applies to rounds
+ * run by the stream driver.  Resets the accumulated phase times. */
+pxr_status pxr_set_profiling(pxr_handle* h, int enable);
+/* Accumulated phase times; writes min(cap, count) entries, sets *count. */
+pxr_status pxr_phase_stats(pxr_handle* h, pxr_phase_stat* out, uint32_t cap, uint32_t* count);
 
 /* Test hooks with no counterpart in the reference: overwrite the potentials
  * (n doubles, rounded to the product's float storage), or the whole round

@@ -22,11 +22,12 @@ DRIVER_STREAM = 1
 # every symbol the header declares, in header order
 SYMBOLS = [
     "pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_create", "pxr_destroy",
-    "pxr_set_stream", "pxr_initialize", "pxr_initialize64", "pxr_walk_step", "pxr_sweep",
+    "pxr_set_stream", "pxr_initialize", "pxr_initialize64", "pxr_initialize_device", "pxr_walk_step", "pxr_sweep",
     "pxr_cut_clusters", "pxr_decompose", "pxr_read_potentials", "pxr_read_sweep_cuts",
     "pxr_download_partition", "pxr_final_partition", "pxr_num_cut_edges", "pxr_download_graph",
     "pxr_download_graph64", "pxr_download_degrees", "pxr_download_labels", "pxr_active_edge_map",
-    "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_potentials", "pxr_set_state",
+    "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
+    "pxr_set_potentials", "pxr_set_state",
 ]
 
 
@@ -48,7 +49,13 @@ class NodeData(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("rounds", C.c_uint32), ("active_vertices", C.c_uint32), ("active_clusters", C.c_uint32),
                 ("clusters_with_cut", C.c_uint32), ("device_bytes", C.c_uint64),
-                ("last_decompose_ms", C.c_double)]
+                ("last_decompose_ms", C.c_double), ("kernel_launches", C.c_uint64),
+                ("walk_vertices", C.c_uint64), ("walk_slots", C.c_uint64), ("walk_gathers", C.c_uint64),
+                ("sort_items", C.c_uint64)]
+
+
+class PhaseStat(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("ms", C.c_double), ("launches", C.c_uint64)]
 
 
 class PxrError(RuntimeError):
@@ -82,6 +89,9 @@ def load() -> C.CDLL:
     L.pxr_set_stream.argtypes = [p, p]
     L.pxr_initialize.argtypes = [p, u32, u64, p, p]
     L.pxr_initialize64.argtypes = [p, u32, u64, p, p]
+    L.pxr_initialize_device.argtypes = [p, u32, u64, p, C.c_int, p]
+    L.pxr_set_profiling.argtypes = [p, C.c_int]
+    L.pxr_phase_stats.argtypes = [p, C.POINTER(PhaseStat), u32, C.POINTER(u32)]
     for name in ["pxr_walk_step", "pxr_sweep", "pxr_cut_clusters"]:
         getattr(L, name).argtypes = [p]
     L.pxr_decompose.argtypes = [p, C.POINTER(u32)]

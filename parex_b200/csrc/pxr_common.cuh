@@ -36,12 +36,18 @@ struct RoundCtr {
     uint32_t full_components; // run components over every cluster in the next cut
     uint32_t err;             // kErr* bits
     uint32_t tile_counter[8]; // dynamic tile ids for look-back kernels
-    uint32_t rounds;          // rounds completed by the device loop
+    uint32_t rounds;          // rounds completed
     uint32_t done;            // set when no active cluster is left
     uint32_t main_sel;        // buffer holding the last sweep's sorted keys and values
     uint32_t sweep_n;         // items of the last sweep
     uint32_t sweep_k;         // clusters of the last sweep
-    uint32_t pad[3];
+    uint32_t loop_start;      // rounds at the start of the device-driven loop
+    uint32_t loop_cap;        // round cap of the device-driven loop
+    uint32_t pad0;
+    unsigned long long stat_walk_vertices;  // traffic counters since initialisation
+    unsigned long long stat_walk_slots;
+    unsigned long long stat_walk_gathers;
+    unsigned long long stat_sort_items;
 };
 
 // ---------------------------------------------------------------------------

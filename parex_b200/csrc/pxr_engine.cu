@@ -107,6 +107,32 @@ __global__ void k_refresh_scaled(const float* x, const uint32_t* ideg, uint32_t 
     if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(xmax_bits, vmax);
 }
 
+// input checks for a CSR already on the device: offsets[0] == 0, offsets[n]
+// == 2m, non-decreasing offsets, columns < n; also the maximum row length.
+template <typename OffT>
+__global__ void k_validate(const OffT* off, const uint32_t* cols, uint32_t n, uint64_t slots, uint32_t* bad,
+                           uint32_t* maxdeg) {
+    uint32_t b = 0, mx = 0;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = tid; v < n; v += stride) {
+        const OffT a = off[v], z = off[v + 1];
+        if (z < a) b |= 1u;
+        else mx = max(mx, (uint32_t)min((uint64_t)(z - a), (uint64_t)0xFFFFFFFFu));
+    }
+    if (tid == 0 && ((uint64_t)off[0] != 0 || (uint64_t)off[n] != slots)) b |= 2u;
+    for (uint64_t j = tid; j < slots; j += stride)
+        if (cols[j] >= n) b |= 4u;
+    for (int o = 16; o > 0; o >>= 1) {
+        b |= __shfl_xor_sync(0xFFFFFFFFu, b, o);
+        mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (b) atomicOr(bad, b);
+        if (mx) atomicMax(maxdeg, mx);
+    }
+}
+
 __global__ void k_bump_site(uint32_t* epoch, RoundCtr* ctr, int site) {
     epoch[site] += 1;
     ctr->tile_counter[site] = 0;
@@ -177,12 +203,20 @@ struct pxr_handle {
     unsigned long long* d_valid = nullptr;
     RoundCtr* h_ctr = nullptr;  // pinned mirror
 
+    uint32_t* d_check = nullptr;   // [2]: invalid-input bits, max row length
     int xcur = 0, tcur = 0, acur = 0;
     int sweep_tab = 0;
-    cudaGraphExec_t graph = nullptr;
-    int graph_parity = -1;
+    cudaGraphExec_t graphs[8] = {};  // device-driven loop, one per parity combination
+    cudaGraphConditionalHandle conds[8] = {};
     uint32_t last_rounds = 0;
     double last_ms = 0.0;
+    uint64_t launches = 0;
+    // per-phase profiling (stream driver)
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    std::vector<cudaEvent_t> event_pool;
+    double phase_ms[16] = {};
+    uint64_t phase_launches[16] = {};
 };
 
 namespace {
@@ -215,9 +249,13 @@ cudaError_t dalloc(pxr_handle* h, T** p, size_t count) {
     return cudaSuccess;
 }
 
+void drop_graphs(pxr_handle* h) {
+    for (auto& g : h->graphs)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
 void release(pxr_handle* h) {
-    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
-    h->graph_parity = -1;
+    drop_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     h->allocs.clear();
     h->bytes = 0;
@@ -266,16 +304,62 @@ Dev<OffT> make_dev(pxr_handle* h) {
 }
 
 // ---------------------------------------------------------------------------
+// phase profiling: CUDA events around each phase of a round (stream driver)
+
+enum Phase {
+    kPhWalk, kPhNodeDiff, kPhEmit, kPhSort, kPhScan, kPhClusterCut, kPhCutInit, kPhUnion,
+    kPhComponents, kPhRootSort, kPhRelabel, kPhApply, kPhDisable, kPhCvol, kPhBook, kPhaseCount
+};
+const char* kPhaseNames[kPhaseCount] = {"walk", "nodediff", "emit_keys", "sort", "sweep_scan", "cluster_cut",
+                                        "cut_init", "union", "components", "root_sort", "relabel", "apply",
+                                        "disable", "cvol_scan", "bookkeeping"};
+
+cudaEvent_t take_event(pxr_handle* h) {
+    if (!h->event_pool.empty()) {
+        cudaEvent_t e = h->event_pool.back();
+        h->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+template <class F>
+void phase(pxr_handle* h, Phase ph, int nlaunch, F&& launch) {
+    h->launches += nlaunch;
+    h->phase_launches[ph] += nlaunch;
+    if (!h->profiling) { launch(); return; }
+    cudaEvent_t a = take_event(h), b = take_event(h);
+    cudaEventRecord(a, h->stream);
+    launch();
+    cudaEventRecord(b, h->stream);
+    h->marks.push_back({ph, {a, b}});
+}
+
+void collect_phases(pxr_handle* h) {
+    for (auto& mk : h->marks) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, mk.second.first, mk.second.second) == cudaSuccess) h->phase_ms[mk.first] += ms;
+        h->event_pool.push_back(mk.second.first);
+        h->event_pool.push_back(mk.second.second);
+    }
+    h->marks.clear();
+}
+
+// ---------------------------------------------------------------------------
 // stages
 
 template <typename OffT, int W>
 cudaError_t op_walk(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
-    k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1);
-    k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
-                                                                      h->xt[h->xcur ^ 1]);
-    k_after_walk<OffT><<<1, 1, 0, s>>>(d);
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1); });
+    phase(h, kPhWalk, 1, [&] {
+        k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
+                                                                          h->xt[h->xcur ^ 1]);
+    });
+    phase(h, kPhBook, 1, [&] { k_after_walk<OffT><<<1, 1, 0, s>>>(d); });
     h->xcur ^= 1;
     return cudaGetLastError();
 }
@@ -285,20 +369,27 @@ cudaError_t op_sweep(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     const ClusterTables& t = h->tab[h->tcur];
-    k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0);
-    k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
-    k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
+    phase(h, kPhNodeDiff, 1, [&] {
+        k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
+    });
+    phase(h, kPhEmit, 1, [&] {
+        k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+    });
     SortBuffers<uint64_t> b{};
     b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
     b.vals[0] = h->vals[0]; b.vals[1] = h->vals[1];
     b.count = &h->ctr->n_active;
     b.end_bit = h->sort_end_bit;
     b.capacity = h->n;
-    cudaError_t e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64);
+    cudaError_t e = cudaSuccess;
+    phase(h, kPhSort, 2 + kMaxPasses, [&] { e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64); });
     if (e != cudaSuccess) return e;
-    const uint32_t tiles = (h->n + kScanTile - 1) / kScanTile;
-    k_sweep_scan<OffT><<<std::max(tiles, 1u), kBlock, 0, s>>>(d, t, h->keys[0], h->keys[1], h->vals[0], h->vals[1]);
-    k_cluster_cut<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t);
+    const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
+    phase(h, kPhScan, 1, [&] {
+        k_sweep_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->keys[0], h->keys[1], h->vals[0], h->vals[1]);
+    });
+    phase(h, kPhClusterCut, 1, [&] { k_cluster_cut<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t); });
     h->sweep_tab = h->tcur;
     return cudaGetLastError();
 }
@@ -310,24 +401,41 @@ cudaError_t op_cut(pxr_handle* h) {
     const ClusterTables& t = h->tab[h->tcur];
     const ClusterTables& nt = h->tab[h->tcur ^ 1];
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
-    k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0);
-    k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
-    k_union<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0],
-                                                                       h->keys[1]);
-    k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0],
-                                                                          h->keys[1], h->roots[0]);
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
+    phase(h, kPhCutInit, 1, [&] {
+        k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
+    });
+    phase(h, kPhUnion, 1, [&] {
+        k_union<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0],
+                                                                           h->keys[1]);
+    });
+    phase(h, kPhComponents, 1, [&] {
+        k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1],
+                                                                              h->keys[0], h->keys[1], h->roots[0]);
+    });
     SortBuffers<uint32_t> rb{};
     rb.keys[0] = h->roots[0]; rb.keys[1] = h->roots[1];
     rb.count = &h->ctr->n_roots;
     rb.end_bit = h->root_end_bit;
     rb.capacity = h->n;
-    cudaError_t e = radix_sort<uint32_t>(rb, h->sort, &h->ctr->err, s, (int)std::max(1u, host_bitlen(h->n)));
+    cudaError_t e = cudaSuccess;
+    const int root_bits = (int)std::max(1u, host_bitlen(h->n));
+    phase(h, kPhRootSort, 2 + (root_bits + 7) / 8, [&] {
+        SortState rs = h->sort;
+        rs.items_moved = nullptr;
+        e = radix_sort<uint32_t>(rb, rs, &h->ctr->err, s, root_bits);
+    });
     if (e != cudaSuccess) return e;
-    k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], h->roots[1], nt);
-    k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1], h->act[h->acur ^ 1]);
-    k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
-    k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt);
-    k_round_end<OffT><<<1, 1, 0, s>>>(d);
+    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], h->roots[1], nt); });
+    phase(h, kPhApply, 1, [&] {
+        k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
+                                               h->act[h->acur ^ 1]);
+    });
+    phase(h, kPhDisable, 1, [&] {
+        k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
+    });
+    phase(h, kPhCvol, 1, [&] { k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt); });
+    phase(h, kPhBook, 1, [&] { k_round_end<OffT><<<1, 1, 0, s>>>(d); });
     h->tcur ^= 1;
     h->acur ^= 1;
     return cudaGetLastError();
@@ -341,16 +449,28 @@ cudaError_t op_round(pxr_handle* h) {
     return e;
 }
 
-enum Op { kOpWalk, kOpSweep, kOpCut, kOpRound };
+// two rounds (the parities return to their start) and the loop condition
+template <typename OffT, int W>
+cudaError_t op_loop_body(pxr_handle* h, cudaGraphConditionalHandle cond) {
+    cudaError_t e = op_round<OffT, W>(h);
+    if (e == cudaSuccess) e = op_round<OffT, W>(h);
+    if (e != cudaSuccess) return e;
+    Dev<OffT> d = make_dev<OffT>(h);
+    phase(h, kPhBook, 1, [&] { k_loop_cond<OffT><<<1, 1, 0, h->stream>>>(d, cond); });
+    return cudaGetLastError();
+}
+
+enum Op { kOpWalk, kOpSweep, kOpCut, kOpRound, kOpLoopBody };
 
 template <typename OffT>
-cudaError_t dispatch_w(pxr_handle* h, Op op) {
-#define PXR_OPS(WV)                                      \
-    switch (op) {                                        \
-        case kOpWalk: return op_walk<OffT, WV>(h);       \
-        case kOpSweep: return op_sweep<OffT, WV>(h);     \
-        case kOpCut: return op_cut<OffT, WV>(h);         \
-        default: return op_round<OffT, WV>(h);           \
+cudaError_t dispatch_w(pxr_handle* h, Op op, cudaGraphConditionalHandle cond) {
+#define PXR_OPS(WV)                                              \
+    switch (op) {                                                \
+        case kOpWalk: return op_walk<OffT, WV>(h);               \
+        case kOpSweep: return op_sweep<OffT, WV>(h);             \
+        case kOpCut: return op_cut<OffT, WV>(h);                 \
+        case kOpLoopBody: return op_loop_body<OffT, WV>(h, cond); \
+        default: return op_round<OffT, WV>(h);                   \
     }
     switch (h->W) {
         case 4: PXR_OPS(4)
@@ -361,8 +481,8 @@ cudaError_t dispatch_w(pxr_handle* h, Op op) {
 #undef PXR_OPS
 }
 
-cudaError_t dispatch(pxr_handle* h, Op op) {
-    return h->off64 ? dispatch_w<uint64_t>(h, op) : dispatch_w<uint32_t>(h, op);
+cudaError_t dispatch(pxr_handle* h, Op op, cudaGraphConditionalHandle cond = 0) {
+    return h->off64 ? dispatch_w<uint64_t>(h, op, cond) : dispatch_w<uint32_t>(h, op, cond);
 }
 
 pxr_status check_device_errors(pxr_handle* h) {
@@ -378,6 +498,7 @@ pxr_status check_device_errors(pxr_handle* h) {
 pxr_status sync_ctr(pxr_handle* h) {
     PXR_CUDA(h, cudaMemcpyAsync(h->h_ctr, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, h->stream));
     PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    collect_phases(h);
     return check_device_errors(h);
 }
 
@@ -387,6 +508,72 @@ pxr_status run_op(pxr_handle* h, Op op) {
     cudaError_t e = dispatch(h, op);
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     return sync_ctr(h);
+}
+
+// Capture the two-round loop body under a conditional while node; the whole
+// decomposition then runs as one graph launch with no host round trip.
+pxr_status build_loop_graph(pxr_handle* h, int key) {
+    cudaGraph_t g = nullptr;
+    PXR_CUDA(h, cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond = 0;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1u, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(h, e, "cudaGraphConditionalHandleCreate"); }
+    cudaGraphNodeParams params{};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = cond;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &params);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(h, e, "cudaGraphAddNode(conditional)"); }
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    cudaStream_t user = h->stream;
+    h->stream = h->own_stream;
+    const bool prof = h->profiling;
+    h->profiling = false;
+    e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    cudaError_t e2 = e == cudaSuccess ? dispatch(h, kOpLoopBody, cond) : e;
+    cudaGraph_t captured = nullptr;
+    if (e == cudaSuccess) e = cudaStreamEndCapture(h->stream, &captured);
+    h->stream = user;
+    h->profiling = prof;
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(h, e, "round capture"); }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaGraphInstantiate");
+    h->graphs[key] = exec;
+    h->conds[key] = cond;
+    return PXR_OK;
+}
+
+__global__ void k_loop_begin(RoundCtr* c, uint32_t cap) {
+    c->loop_start = c->rounds;
+    c->loop_cap = cap;
+}
+
+pxr_status decompose_graph(pxr_handle* h) {
+    const int key = h->xcur | (h->tcur << 1) | (h->acur << 2);
+    if (!h->graphs[key]) {
+        pxr_status st = build_loop_graph(h, key);
+        if (st != PXR_OK) return st;
+    }
+    k_loop_begin<<<1, 1, 0, h->stream>>>(h->ctr, h->cfg.max_rounds);
+    PXR_CUDA(h, cudaGetLastError());
+    PXR_CUDA(h, cudaGraphLaunch(h->graphs[key], h->stream));
+    return sync_ctr(h);
+}
+
+pxr_status decompose_stream(pxr_handle* h) {
+    pxr_status st = sync_ctr(h);
+    const uint32_t start = h->h_ctr->rounds;
+    while (st == PXR_OK && !h->h_ctr->done && h->h_ctr->rounds - start < h->cfg.max_rounds) {
+        cudaError_t e = dispatch(h, kOpRound);
+        if (e != cudaSuccess) return cuda_fail(h, e, "round launch");
+        st = sync_ctr(h);
+    }
+    return st;
 }
 
 // ---------------------------------------------------------------------------
@@ -405,31 +592,12 @@ pxr_status setup_tables_initial(pxr_handle* h) {
 }
 
 template <typename OffT>
-pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* offsets, const uint32_t* cols) {
-    if (!h) return PXR_INVALID_ARG;
-    if (!offsets || (m > 0 && !cols)) return fail(h, PXR_INVALID_ARG, "null graph pointer");
-    if (n >= 0x7FFFFFFFu) return fail(h, PXR_INVALID_ARG, "n must be below 2^31 - 1");
-    if ((uint64_t)offsets[0] != 0 || (uint64_t)offsets[n] != 2 * m)
-        return fail(h, PXR_INVALID_ARG, "offsets must start at 0 and end at 2m");
-    uint64_t maxdeg = 0;
-    for (uint32_t v = 0; v < n; ++v) {
-        if (offsets[v + 1] < offsets[v]) return fail(h, PXR_INVALID_ARG, "offsets must be non-decreasing");
-        maxdeg = std::max<uint64_t>(maxdeg, (uint64_t)(offsets[v + 1] - offsets[v]));
-    }
-    for (uint64_t j = 0; j < 2 * m; ++j)
-        if (cols[j] >= n) return fail(h, PXR_INVALID_ARG, "column index out of range");
-    PXR_CUDA(h, cudaSetDevice(h->device));
+pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     release(h);
     h->n = n;
     h->m = m;
     h->slots = 2 * m;
-    h->maxdeg = (uint32_t)maxdeg;
     h->off64 = sizeof(OffT) == 8;
-    h->nb_bits = host_bitlen(std::max<uint64_t>(n, maxdeg));
-    // lanes per vertex: the power of two nearest the mean degree, 4..32
-    const double mean = n ? (double)(2 * m) / n : 0.0;
-    h->W = mean <= 6.0 ? 4u : mean <= 12.0 ? 8u : mean <= 24.0 ? 16u : 32u;
-    h->xcur = h->tcur = h->acur = 0;
     const size_t N = std::max<uint32_t>(n, 1);
     const uint32_t scan_tiles = (uint32_t)((N + kScanTile - 1) / kScanTile) + 1;
     const uint32_t sort_tiles = (uint32_t)((N + kSortTile - 1) / kSortTile) + 1;
@@ -452,42 +620,85 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     A(&h->sort.pass_info, kMaxPasses + 1); A(&h->sort.tile_ctr, kMaxPasses); A(&h->sort.epoch, 1);
     A(&h->sort.status, (size_t)sort_tiles * kRadix);
     A(&h->sort_end_bit, 1); A(&h->root_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
-    A(&h->d_num, 1); A(&h->d_valid, 1);
+    A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 2);
 #undef A
     if (e != cudaSuccess) { release(h); return cuda_fail(h, e, "cudaMalloc"); }
     h->sort.max_tiles = sort_tiles;
+    h->sort.items_moved = &h->ctr->stat_sort_items;
+    // look-back flags and sort status words carry epochs that only grow, so
+    // they are cleared once here and never again
     cudaStream_t s = h->stream;
-    PXR_CUDA(h, cudaMemcpyAsync(h->off, offsets, ((size_t)n + 1) * sizeof(OffT), cudaMemcpyHostToDevice, s));
-    if (m) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, cudaMemcpyHostToDevice, s));
-    for (int i = 0; i < 6; ++i) {
-        PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
-    }
+    for (int i = 0; i < 6; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, 8 * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->ctr, 0, sizeof(RoundCtr), s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.hist, 0, kMaxPasses * kRadix * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.epoch, 0, 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.status, 0, (size_t)sort_tiles * kRadix * 8, s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.pass_info, 0, (kMaxPasses + 1) * 4, s));
-    const uint32_t consts[4] = {host_bitlen(n > 0 ? n - 1 : 0), 32u, n, 0u};
+    const uint32_t consts[3] = {host_bitlen(n > 0 ? n - 1 : 0), 32u, n};
     PXR_CUDA(h, cudaMemcpyAsync(h->root_end_bit, &consts[0], 4, cudaMemcpyHostToDevice, s));
     PXR_CUDA(h, cudaMemcpyAsync(h->fp_end_bit, &consts[1], 4, cudaMemcpyHostToDevice, s));
     PXR_CUDA(h, cudaMemcpyAsync(h->d_n, &consts[2], 4, cudaMemcpyHostToDevice, s));
+    return PXR_OK;
+}
+
+// offsets/cols: host pointers (kind = cudaMemcpyHostToDevice) or device pointers
+template <typename OffT>
+pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* offsets, const uint32_t* cols,
+                           cudaMemcpyKind kind) {
+    if (!h) return PXR_INVALID_ARG;
+    if (!offsets || (m > 0 && !cols)) return fail(h, PXR_INVALID_ARG, "null graph pointer");
+    if (n >= 0x7FFFFFFFu) return fail(h, PXR_INVALID_ARG, "n must be below 2^31 - 1");
+    PXR_CUDA(h, cudaSetDevice(h->device));
+    h->initialized = false;
+    const bool reuse = !h->allocs.empty() && h->n == n && h->m == m && h->off64 == (sizeof(OffT) == 8);
+    if (!reuse) {
+        pxr_status st = allocate<OffT>(h, n, m);
+        if (st != PXR_OK) return st;
+    }
+    cudaStream_t s = h->stream;
+    h->xcur = h->tcur = h->acur = 0;
+    PXR_CUDA(h, cudaMemcpyAsync(h->off, offsets, ((size_t)n + 1) * sizeof(OffT), kind, s));
+    if (m) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, kind, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->d_check, 0, 8, s));
+    k_validate<OffT><<<grid_for(std::max<uint64_t>(h->slots, n)), kBlock, 0, s>>>(
+        static_cast<const OffT*>(h->off), h->cols, n, h->slots, &h->d_check[0], &h->d_check[1]);
+    ++h->launches;
+    uint32_t check[2] = {0, 0};
+    PXR_CUDA(h, cudaMemcpyAsync(check, h->d_check, 8, cudaMemcpyDeviceToHost, s));
+    PXR_CUDA(h, cudaStreamSynchronize(s));
+    if (check[0] & 2u) return fail(h, PXR_INVALID_ARG, "offsets must start at 0 and end at 2m");
+    if (check[0] & 1u) return fail(h, PXR_INVALID_ARG, "offsets must be non-decreasing");
+    if (check[0] & 4u) return fail(h, PXR_INVALID_ARG, "column index out of range");
+    h->maxdeg = check[1];
+    const uint32_t nb_bits = host_bitlen(std::max<uint64_t>(n, h->maxdeg));
+    // lanes per vertex: the power of two nearest the mean degree, 4..32
+    const double mean = n ? (double)(2 * m) / n : 0.0;
+    const uint32_t W = mean <= 6.0 ? 4u : mean <= 12.0 ? 8u : mean <= 24.0 ? 16u : 32u;
+    // captured round graphs bake in buffers, nb_bits and W: keep them only if all are unchanged
+    if (!reuse || nb_bits != h->nb_bits || W != h->W) drop_graphs(h);
+    h->nb_bits = nb_bits;
+    h->W = W;
+    // round state: one cluster, every vertex active; keep the growing epochs
+    RoundCtr c;
+    PXR_CUDA(h, cudaMemcpyAsync(&c, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, s));
+    PXR_CUDA(h, cudaStreamSynchronize(s));
+    const RoundCtr old = c;
+    std::memset(&c, 0, sizeof(c));
+    c.n_active = n;
+    c.n_clusters = n ? 1u : 0u;
+    c.full_components = 1;
+    c.done = n ? 0u : 1u;
+    c.main_sel = old.main_sel;
+    PXR_CUDA(h, cudaMemcpyAsync(h->ctr, &c, sizeof(RoundCtr), cudaMemcpyHostToDevice, s));
     if (n) {
         k_degrees<OffT><<<grid_for(n), kBlock, 0, s>>>(static_cast<const OffT*>(h->off), n, h->ideg, h->lab,
                                                       h->act[0], h->ids[0]);
         launch_initial_potentials(h->off, h->off64, n, h->cfg.seed, h->x, &h->ctr->xmax_bits, s);
         k_refresh_scaled<<<grid_for(n), kBlock, 0, s>>>(h->x, h->ideg, n, h->xt[0], &h->ctr->xmax_bits);
+        PXR_CUDA(h, cudaMemcpyAsync(&h->ctr->xmax_walk_bits, &h->ctr->xmax_bits, 4, cudaMemcpyDeviceToDevice, s));
+        h->launches += 3;
     }
-    RoundCtr c{};
-    c.n_active = n;
-    c.n_clusters = n ? 1u : 0u;
-    c.smallest = 0;
-    c.full_components = 1;
-    c.done = n ? 0u : 1u;
-    // everything but xmax_bits, which the kernels above produce
-    PXR_CUDA(h, cudaMemcpyAsync(h->ctr, &c, offsetof(RoundCtr, xmax_bits), cudaMemcpyHostToDevice, s));
-    PXR_CUDA(h, cudaMemcpyAsync(&h->ctr->full_components, &c.full_components,
-                                sizeof(RoundCtr) - offsetof(RoundCtr, full_components), cudaMemcpyHostToDevice, s));
     pxr_status st = setup_tables_initial(h);
     if (st != PXR_OK) return st;
     PXR_CUDA(h, cudaGetLastError());
@@ -568,6 +779,8 @@ void pxr_destroy(pxr_handle* h) {
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     release(h);
+    collect_phases(h);
+    for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
     if (h->h_ctr) cudaFreeHost(h->h_ctr);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
@@ -575,24 +788,31 @@ void pxr_destroy(pxr_handle* h) {
 
 pxr_status pxr_set_stream(pxr_handle* h, void* stream) {
     if (!h) return PXR_INVALID_ARG;
-    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_parity = -1; }
     h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
     return PXR_OK;
 }
 
 pxr_status pxr_initialize(pxr_handle* h, uint32_t n, uint64_t m, const uint32_t* offsets, const uint32_t* cols) {
     if (2 * m >= (1ull << 32)) return fail(h, PXR_INVALID_ARG, "32-bit offsets need 2m < 2^32");
-    return initialize_impl<uint32_t>(h, n, m, offsets, cols);
+    return initialize_impl<uint32_t>(h, n, m, offsets, cols, cudaMemcpyHostToDevice);
 }
 
 pxr_status pxr_initialize64(pxr_handle* h, uint32_t n, uint64_t m, const uint64_t* offsets, const uint32_t* cols) {
-    if (2 * m < (1ull << 32)) {
+    if (offsets && 2 * m < (1ull << 32)) {
         // keep 32-bit offsets on the device when they fit: half the offset traffic
         std::vector<uint32_t> o32((size_t)n + 1);
         for (size_t i = 0; i <= n; ++i) o32[i] = (uint32_t)offsets[i];
-        return initialize_impl<uint32_t>(h, n, m, o32.data(), cols);
+        return initialize_impl<uint32_t>(h, n, m, o32.data(), cols, cudaMemcpyHostToDevice);
     }
-    return initialize_impl<uint64_t>(h, n, m, offsets, cols);
+    return initialize_impl<uint64_t>(h, n, m, offsets, cols, cudaMemcpyHostToDevice);
+}
+
+pxr_status pxr_initialize_device(pxr_handle* h, uint32_t n, uint64_t m, const void* offsets, int offsets_are_64bit,
+                                 const uint32_t* cols) {
+    if (offsets_are_64bit)
+        return initialize_impl<uint64_t>(h, n, m, static_cast<const uint64_t*>(offsets), cols, cudaMemcpyDeviceToDevice);
+    if (2 * m >= (1ull << 32)) return fail(h, PXR_INVALID_ARG, "32-bit offsets need 2m < 2^32");
+    return initialize_impl<uint32_t>(h, n, m, static_cast<const uint32_t*>(offsets), cols, cudaMemcpyDeviceToDevice);
 }
 
 pxr_status pxr_walk_step(pxr_handle* h) { return run_op(h, kOpWalk); }
@@ -608,12 +828,7 @@ pxr_status pxr_decompose(pxr_handle* h, uint32_t* rounds_out) {
     pxr_status st = sync_ctr(h);
     const uint32_t start_rounds = h->h_ctr->rounds;
     PXR_CUDA(h, cudaEventRecord(e0, h->stream));
-    const uint32_t cap = h->cfg.max_rounds;
-    while (st == PXR_OK && !h->h_ctr->done && h->h_ctr->rounds - start_rounds < cap) {
-        cudaError_t e = dispatch(h, kOpRound);
-        if (e != cudaSuccess) { st = cuda_fail(h, e, "round launch"); break; }
-        st = sync_ctr(h);
-    }
+    if (st == PXR_OK) st = h->cfg.driver == PXR_DRIVER_GRAPH ? decompose_graph(h) : decompose_stream(h);
     PXR_CUDA(h, cudaEventRecord(e1, h->stream));
     PXR_CUDA(h, cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -696,6 +911,7 @@ pxr_status pxr_final_partition(pxr_handle* h, int32_t* ids, int32_t* num_cluster
     uint32_t* v1 = h->ids[h->acur ^ 1];
     int32_t* out = reinterpret_cast<int32_t*>(h->dv);
     k_fp_keys<<<grid_for(n), kBlock, 0, s>>>(h->lab, n, k0, v0);
+    h->launches += 4 + 2 + 4;
     SortBuffers<uint32_t> b{};
     b.keys[0] = k0; b.keys[1] = k1; b.vals[0] = v0; b.vals[1] = v1;
     b.count = h->d_n;
@@ -792,12 +1008,37 @@ pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out) {
     out->device_bytes = h->bytes;
     out->rounds = h->last_rounds;
     out->last_decompose_ms = h->last_ms;
+    out->kernel_launches = h->launches;
     if (!h->initialized) return PXR_OK;
     pxr_status st = sync_ctr(h);
     out->active_vertices = h->h_ctr->n_active;
     out->active_clusters = h->h_ctr->n_clusters;
     out->clusters_with_cut = h->h_ctr->n_cut;
+    out->walk_vertices = h->h_ctr->stat_walk_vertices;
+    out->walk_slots = h->h_ctr->stat_walk_slots;
+    out->walk_gathers = h->h_ctr->stat_walk_gathers;
+    out->sort_items = h->h_ctr->stat_sort_items;
     return st;
+}
+
+pxr_status pxr_set_profiling(pxr_handle* h, int enable) {
+    if (!h) return PXR_INVALID_ARG;
+    h->profiling = enable != 0;
+    std::memset(h->phase_ms, 0, sizeof(h->phase_ms));
+    std::memset(h->phase_launches, 0, sizeof(h->phase_launches));
+    return PXR_OK;
+}
+
+pxr_status pxr_phase_stats(pxr_handle* h, pxr_phase_stat* out, uint32_t cap, uint32_t* count) {
+    if (!h || !count) return PXR_INVALID_ARG;
+    *count = kPhaseCount;
+    for (uint32_t i = 0; i < std::min<uint32_t>(cap, kPhaseCount) && out; ++i) {
+        std::memset(&out[i], 0, sizeof(out[i]));
+        std::strncpy(out[i].name, kPhaseNames[i], sizeof(out[i].name) - 1);
+        out[i].ms = h->phase_ms[i];
+        out[i].launches = h->phase_launches[i];
+    }
+    return PXR_OK;
 }
 
 pxr_status pxr_set_potentials(pxr_handle* h, const double* x) {
@@ -806,11 +1047,14 @@ pxr_status pxr_set_potentials(pxr_handle* h, const double* x) {
     std::vector<float> xf(h->n);
     for (uint32_t v = 0; v < h->n; ++v) xf[v] = (float)x[v];
     PXR_CUDA(h, cudaMemcpyAsync(h->x, xf.data(), (size_t)h->n * 4, cudaMemcpyHostToDevice, h->stream));
-    PXR_CUDA(h, cudaMemsetAsync(&h->ctr->xmax_bits, 0, 4, h->stream));
+    // the walk and the per-cluster sums both take their fixed-point scale from
+    // the max |x| over every vertex, as after initialisation
+    PXR_CUDA(h, cudaMemsetAsync(&h->ctr->xmax_bits, 0, 8, h->stream));
     if (h->n)
         k_refresh_scaled<<<grid_for(h->n), kBlock, 0, h->stream>>>(h->x, h->ideg, h->n, h->xt[h->xcur],
                                                                     &h->ctr->xmax_bits);
     PXR_CUDA(h, cudaGetLastError());
+    PXR_CUDA(h, cudaMemcpyAsync(&h->ctr->xmax_walk_bits, &h->ctr->xmax_bits, 4, cudaMemcpyDeviceToDevice, h->stream));
     return sync_ctr(h);
 }
 

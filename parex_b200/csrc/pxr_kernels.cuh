@@ -166,6 +166,14 @@ __global__ void k_round_end(Dev<OffT> d) {
     c->done = (c->n_active == 0 || c->n_clusters == 0) ? 1u : 0u;
 }
 
+// device-driven round loop: keep looping while clusters remain and the cap allows
+template <typename OffT>
+__global__ void k_loop_cond(Dev<OffT> d, cudaGraphConditionalHandle cond) {
+    const RoundCtr* c = d.ctr;
+    const bool more = !c->done && c->err == 0 && (c->rounds - c->loop_start) < c->loop_cap;
+    cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
 // ---------------------------------------------------------------------------
 // walk: x'[v] = 0.9 * sum_{u ~ v, valid} x[u]/d(u) + 0.1 * x[v]
 // (fusedRandomWalk_WarpParallel, cuda/devRandomWalk.h:117-203), W lanes per
@@ -181,6 +189,7 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
     const uint32_t groups = (gridDim.x * blockDim.x) / W;
     const uint32_t warp0 = ((blockIdx.x * blockDim.x + threadIdx.x) & ~31u) / W;
     uint32_t vmax = 0;
+    unsigned long long st_v = 0, st_s = 0, st_g = 0;
     for (uint32_t j0 = warp0; j0 < count; j0 += groups) {
         const uint32_t j = j0 + (threadIdx.x & 31u) / W;
         const bool valid = j < count;
@@ -189,8 +198,10 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
         int64_t acc = 0;
         for (OffT s = beg + gl; s < end; s += W) {
             const uint32_t nb = d.cols[s];
-            if (nb != kInvalidEdge) acc += to_fixed(xt_in[nb], scale);
+            ++st_s;
+            if (nb != kInvalidEdge) { acc += to_fixed(xt_in[nb], scale); ++st_g; }
         }
+        st_v += (valid && gl == 0) ? 1 : 0;
 #pragma unroll
         for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o, W);
         if (valid && gl == 0) {
@@ -205,8 +216,20 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
         }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
-    if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
+    for (int o = 16; o > 0; o >>= 1) {
+        vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+        st_v += __shfl_xor_sync(0xFFFFFFFFu, st_v, o);
+        st_s += __shfl_xor_sync(0xFFFFFFFFu, st_s, o);
+        st_g += __shfl_xor_sync(0xFFFFFFFFu, st_g, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
+        if (st_v) {
+            atomicAdd(&d.ctr->stat_walk_vertices, st_v);
+            atomicAdd(&d.ctr->stat_walk_slots, st_s);
+            atomicAdd(&d.ctr->stat_walk_gathers, st_g);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

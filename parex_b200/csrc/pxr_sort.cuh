@@ -33,6 +33,7 @@ struct SortState {
     uint32_t* epoch;      // [1]
     uint64_t* status;     // [max_tiles][kRadix]
     uint32_t max_tiles;
+    unsigned long long* items_moved;  // optional: += items x active passes
 };
 
 template <typename K>
@@ -95,6 +96,9 @@ __global__ void __launch_bounds__(kRadix) sort_plan_kernel(SortBuffers<K> b, Sor
     if (d == 0) {
         s.pass_info[kMaxPasses] = parity;
         *s.epoch = *s.epoch + kMaxPasses;
+        uint32_t active = 0;
+        for (int p = 0; p < kMaxPasses; ++p) active += s.pass_info[p] & 1u;
+        if (s.items_moved) *s.items_moved += (unsigned long long)count * active;
     }
 }
 

@@ -185,6 +185,22 @@ class CudaDeviceManager:
         """No-op, as GraphManager::updateLabels is in the reference."""
 
     # -- extras -----------------------------------------------------------
+    def initialize_device(self, n: int, m: int, offsets_ptr: int, offsets_are_64bit: bool, cols_ptr: int) -> None:
+        """initialize() from a CSR already in device memory (raw device pointers)."""
+        self._call(self._L.pxr_initialize_device, n, m, C.c_void_p(offsets_ptr), 1 if offsets_are_64bit else 0,
+                   C.c_void_p(cols_ptr))
+        self.n, self.m = n, m
+
+    def set_profiling(self, enable: bool) -> None:
+        self._call(self._L.pxr_set_profiling, 1 if enable else 0)
+
+    def phase_stats(self) -> list[dict]:
+        count = C.c_uint32(0)
+        self._call(self._L.pxr_phase_stats, None, 0, C.byref(count))
+        arr = (_lib.PhaseStat * count.value)()
+        self._call(self._L.pxr_phase_stats, arr, count.value, C.byref(count))
+        return [{"name": a.name.decode(), "ms": a.ms, "launches": a.launches} for a in arr]
+
     def stats(self) -> dict:
         st = _lib.Stats()
         self._call(self._L.pxr_get_stats, C.byref(st))
