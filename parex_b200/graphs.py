@@ -299,6 +299,18 @@ def read_pxg(path: str | os.PathLike) -> CSRGraph:
     return CSRGraph(offsets, cols, os.path.basename(str(path)))
 
 
+def write_mtx(path: str | os.PathLike, g: CSRGraph) -> None:
+    """Matrix Market coordinate file, each undirected edge once, 1-based ids:
+    the input format of the reference's readDynGraph (lib/utils/graph_io.h:49-84)."""
+    src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(g.offsets.astype(np.int64)))
+    keep = src < g.cols
+    u, v = src[keep] + 1, g.cols[keep].astype(np.int64) + 1
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate pattern symmetric\n")
+        f.write(f"{g.n} {g.n} {u.shape[0]}\n")
+        np.savetxt(f, np.stack([u, v], axis=1), fmt="%d")
+
+
 def by_name(name: str) -> CSRGraph:
     """Named workloads: ``sbm16k``, ``grid<side>``, ``rmat<scale>``, ``regular<log2n>``."""
     if name == "sbm16k":
