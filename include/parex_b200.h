@@ -171,6 +171,32 @@ pxr_status pxr_set_profiling(pxr_handle* h, int enable);
 /* Accumulated phase times; writes min(cap, count) entries, sets *count. */
 pxr_status pxr_phase_stats(pxr_handle* h, pxr_phase_stat* out, uint32_t cap, uint32_t* count);
 
+/* Final partition for callers that cannot allocate device memory.  No
+ * counterpart in the reference.
+ *
+ * Some callers may not call cudaMalloc/cudaFree where they need the cluster
+ * ids: their device memory is owned by a pooling allocator that must account
+ * for every byte, or they cannot afford the device-wide synchronisation those
+ * calls may imply.  This entry point allocates nothing: labels (n int32) is
+ * the caller's device array of cluster labels, as pxr_download_labels returns
+ * them; ids (n int32) and num_clusters (one int32) are the caller's device
+ * outputs, filled exactly as pxr_final_partition fills its host outputs
+ * (dense ids ordered by label value).  Work is enqueued on `stream` (a
+ * cudaStream_t as void*, NULL for the legacy default stream) and the call
+ * returns without waiting.
+ *
+ * Limit: n <= PXR_STATIC_SCRATCH_MAX_LABELS; larger n returns
+ * PXR_INVALID_ARG (use pxr_final_partition).  The working memory is a fixed
+ * ~1.1 MB array inside the library, held on every GPU that loads it until
+ * the process exits.  The first call on each device looks up that array's
+ * device address (cudaGetSymbolAddress) with the device current; make that
+ * first call before any stream capture.  All calls share the array: calls
+ * whose work may overlap on the GPU race and must be ordered by the caller.
+ * *num_clusters is -1 if a device-side bounded wait ran out. */
+#define PXR_STATIC_SCRATCH_MAX_LABELS 65536u
+pxr_status pxr_final_partition_static(const int32_t* labels, uint32_t n, int32_t* ids,
+                                      int32_t* num_clusters, void* stream);
+
 /* Test hooks with no counterpart in the reference: overwrite the potentials
  * (n doubles, rounded to the product's float storage), or the whole round
  * state.  act holds the n_act active vertex ids in the order their keys are

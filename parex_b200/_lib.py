@@ -27,8 +27,9 @@ SYMBOLS = [
     "pxr_download_partition", "pxr_final_partition", "pxr_num_cut_edges", "pxr_download_graph",
     "pxr_download_graph64", "pxr_download_degrees", "pxr_download_labels", "pxr_active_edge_map",
     "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
-    "pxr_set_potentials", "pxr_set_state",
+    "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state",
 ]
+STATIC_SCRATCH_MAX_LABELS = 65536
 
 
 class Config(C.Structure):
@@ -107,6 +108,7 @@ def load() -> C.CDLL:
     L.pxr_active_edge_map.argtypes = [p, p]
     L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]
     L.pxr_get_stats.argtypes = [p, C.POINTER(Stats)]
+    L.pxr_final_partition_static.argtypes = [p, u32, p, p, p]
     L.pxr_set_potentials.argtypes = [p, p]
     L.pxr_set_state.argtypes = [p, p, p, u32, p, p, p, u32, i32, C.c_int]
     for name in SYMBOLS:
