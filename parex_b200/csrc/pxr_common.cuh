@@ -130,28 +130,58 @@ __device__ __forceinline__ void lookback_publish(LookbackState s, uint32_t tile,
     st_release(&s.flags[tile], (epoch << 2) | f);
 }
 
-// Exclusive prefix of tile `tile` (Op::identity() for tile 0).  Bounded waits.
+// Exclusive prefix of tile `tile` (Op::identity() for tile 0), computed by
+// one whole warp: lane i waits for tile - 1 - i (bounded), the nearest
+// predecessor holding an inclusive prefix ends the window, and the lanes up
+// to it are combined.  Windows of 32 tiles repeat until an inclusive prefix
+// (or tile 0) is reached.  Op must be commutative.  Every lane gets the result.
 template <class Op>
 __device__ __forceinline__ uint64_t lookback_exclusive(LookbackState s, uint32_t tile, uint32_t epoch,
                                                        uint32_t* err) {
-    uint64_t excl = Op::identity();
-    bool have = false;
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t want = epoch & 0x3FFFFFFFu;
-    for (int32_t t = (int32_t)tile - 1; t >= 0; --t) {
-        uint32_t w = ld_acquire(&s.flags[t]);
-        uint32_t spins = 0;
-        while ((w >> 2) != want || (w & 3u) == 0u) {
-            if (++spins > kSpinLimit) { atomicOr(err, kErrLookback); return excl; }
-            __nanosleep(32);
-            w = ld_acquire(&s.flags[t]);
+    uint64_t excl = Op::identity();
+    for (int32_t base = (int32_t)tile - 1; base >= 0; base -= 32) {
+        const int32_t t = base - (int32_t)lane;
+        uint32_t f = 2u;               // tiles before 0 act as an empty inclusive prefix
+        uint64_t v = Op::identity();
+        if (t >= 0) {
+            uint32_t w = ld_acquire(&s.flags[t]);
+            uint32_t spins = 0;
+            while ((w >> 2) != want || (w & 3u) == 0u) {
+                if (++spins > kSpinLimit) { atomicOr(err, kErrLookback); w = (want << 2) | 2u; break; }
+                __nanosleep(32);
+                w = ld_acquire(&s.flags[t]);
+            }
+            f = w & 3u;
+            if (spins <= kSpinLimit) v = (f == 2u) ? ld_relaxed64(&s.inc[t]) : ld_relaxed64(&s.agg[t]);
         }
-        const uint32_t f = w & 3u;
-        const uint64_t v = (f == 2u) ? ld_relaxed64(&s.inc[t]) : ld_relaxed64(&s.agg[t]);
-        excl = have ? Op::combine(v, excl) : v;
-        have = true;
-        if (f == 2u) break;
+        const uint32_t inc_lanes = __ballot_sync(0xFFFFFFFFu, f == 2u);
+        const uint32_t stop = inc_lanes ? (uint32_t)(__ffs(inc_lanes) - 1) : 31u;
+        uint64_t part = lane <= stop ? v : Op::identity();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part = Op::combine(part, __shfl_xor_sync(0xFFFFFFFFu, part, o));
+        excl = Op::combine(part, excl);
+        if (inc_lanes) break;
     }
     return excl;
+}
+
+// One tile's part of a decoupled look-back, called by warp 0 of the block:
+// publish the aggregate, look back, publish the inclusive prefix.  Returns the
+// exclusive prefix in every lane of warp 0.
+template <class Op>
+__device__ __forceinline__ uint64_t lookback_tile(LookbackState s, uint32_t tile, uint32_t epoch, uint64_t aggregate,
+                                                  uint32_t* err) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (tile == 0) {
+        if (lane == 0) lookback_publish(s, tile, epoch, 2u, aggregate);
+        return Op::identity();
+    }
+    if (lane == 0) lookback_publish(s, tile, epoch, 1u, aggregate);
+    const uint64_t ex = lookback_exclusive<Op>(s, tile, epoch, err);
+    if (lane == 0) lookback_publish(s, tile, epoch, 2u, Op::combine(ex, aggregate));
+    return ex;
 }
 
 // lane-wise addition of two packed uint32 lanes

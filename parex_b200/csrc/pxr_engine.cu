@@ -52,17 +52,10 @@ __global__ void __launch_bounds__(kBlock) k_fp_rank(const uint32_t* keys0, const
     }
     uint64_t total;
     const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &total);
-    if (threadIdx.x == 0) {
-        uint64_t ex = 0;
-        if (tile == 0) {
-            lookback_publish(lb, tile, epoch, 2u, total);
-        } else {
-            lookback_publish(lb, tile, epoch, 1u, total);
-            ex = lookback_exclusive<Add64>(lb, tile, epoch, &ctr->err);
-            lookback_publish(lb, tile, epoch, 2u, ex + total);
-        }
-        s_excl = ex;
-        if (tile == ntiles - 1) *num_out = (int32_t)(ex + total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(lb, tile, epoch, total, &ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
+        if (threadIdx.x == 0 && tile == ntiles - 1) *num_out = (int32_t)(ex + total);
     }
     __syncthreads();
     uint32_t r = (uint32_t)(s_excl + incl - run);
@@ -111,14 +104,18 @@ __global__ void k_refresh_scaled(const float* x, const uint32_t* ideg, uint32_t 
 // == 2m, non-decreasing offsets, columns < n; also the maximum row length.
 template <typename OffT>
 __global__ void k_validate(const OffT* off, const uint32_t* cols, uint32_t n, uint64_t slots, uint32_t* bad,
-                           uint32_t* maxdeg) {
+                           uint32_t* maxdeg, uint32_t* heavy, uint32_t* n_heavy) {
     uint32_t b = 0, mx = 0;
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t v = tid; v < n; v += stride) {
         const OffT a = off[v], z = off[v + 1];
         if (z < a) b |= 1u;
-        else mx = max(mx, (uint32_t)min((uint64_t)(z - a), (uint64_t)0xFFFFFFFFu));
+        else {
+            const uint64_t len = (uint64_t)(z - a);
+            mx = max(mx, (uint32_t)min(len, (uint64_t)0xFFFFFFFFu));
+            if (len > kHeavyRow) heavy[atomicAdd(n_heavy, 1u)] = (uint32_t)v;   // list order is irrelevant
+        }
     }
     if (tid == 0 && ((uint64_t)off[0] != 0 || (uint64_t)off[n] != slots)) b |= 2u;
     for (uint64_t j = tid; j < slots; j += stride)
@@ -131,6 +128,13 @@ __global__ void k_validate(const OffT* off, const uint32_t* cols, uint32_t n, ui
         if (b) atomicOr(bad, b);
         if (mx) atomicMax(maxdeg, mx);
     }
+}
+
+// Profiling aid: hold the stream for a moment so the host can queue a whole
+// op before the device starts it; the phase events then time device work
+// rather than host launch latency.
+__global__ void k_hold(uint32_t ns) {
+    for (uint32_t t = 0; t < ns; t += 1000) __nanosleep(1000);
 }
 
 __global__ void k_bump_site(uint32_t* epoch, RoundCtr* ctr, int site) {
@@ -203,11 +207,14 @@ struct pxr_handle {
     unsigned long long* d_valid = nullptr;
     RoundCtr* h_ctr = nullptr;  // pinned mirror
 
-    uint32_t* d_check = nullptr;   // [2]: invalid-input bits, max row length
+    uint32_t* d_check = nullptr;   // [3]: invalid-input bits, max row length, heavy rows
+    uint32_t* heavy = nullptr;     // vertices with more than kHeavyRow slots
+    uint32_t n_heavy = 0;
     int xcur = 0, tcur = 0, acur = 0;
     int sweep_tab = 0;
     cudaGraphExec_t graphs[8] = {};  // device-driven loop, one per parity combination
     cudaGraphConditionalHandle conds[8] = {};
+    uint64_t body_launches[8] = {};  // kernels per replay of the loop body
     uint32_t last_rounds = 0;
     double last_ms = 0.0;
     uint64_t launches = 0;
@@ -300,6 +307,8 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.sort = h->sort;
     d.sort_end_bit = h->sort_end_bit;
     d.root_end_bit = h->root_end_bit;
+    d.heavy = h->heavy;
+    d.n_heavy = h->n_heavy;
     return d;
 }
 
@@ -350,14 +359,21 @@ void collect_phases(pxr_handle* h) {
 // ---------------------------------------------------------------------------
 // stages
 
+void hold_for_profiling(pxr_handle* h) {
+    if (h->profiling) k_hold<<<1, 1, 0, h->stream>>>(300000u);
+}
+
 template <typename OffT, int W>
 cudaError_t op_walk(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
+    hold_for_profiling(h);
     phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1); });
-    phase(h, kPhWalk, 1, [&] {
+    const uint32_t hgrid = std::min(h->n_heavy, 148u * 16u);
+    phase(h, kPhWalk, h->n_heavy ? 2 : 1, [&] {
         k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
                                                                           h->xt[h->xcur ^ 1]);
+        if (h->n_heavy) k_walk_heavy<OffT><<<hgrid, kBlock, 0, s>>>(d, h->xt[h->xcur], h->xt[h->xcur ^ 1]);
     });
     phase(h, kPhBook, 1, [&] { k_after_walk<OffT><<<1, 1, 0, s>>>(d); });
     h->xcur ^= 1;
@@ -369,9 +385,11 @@ cudaError_t op_sweep(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     const ClusterTables& t = h->tab[h->tcur];
+    hold_for_profiling(h);
     phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
-    phase(h, kPhNodeDiff, 1, [&] {
+    phase(h, kPhNodeDiff, h->n_heavy ? 2 : 1, [&] {
         k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        if (h->n_heavy) k_nodediff_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d);
     });
     phase(h, kPhEmit, 1, [&] {
         k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
@@ -401,13 +419,17 @@ cudaError_t op_cut(pxr_handle* h) {
     const ClusterTables& t = h->tab[h->tcur];
     const ClusterTables& nt = h->tab[h->tcur ^ 1];
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
+    hold_for_profiling(h);
     phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
     phase(h, kPhCutInit, 1, [&] {
         k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });
-    phase(h, kPhUnion, 1, [&] {
+    phase(h, kPhUnion, h->n_heavy ? 4 : 3, [&] {
+        k_link_first<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
+        k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
         k_union<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0],
                                                                            h->keys[1]);
+        if (h->n_heavy) k_union_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d);
     });
     phase(h, kPhComponents, 1, [&] {
         k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1],
@@ -431,8 +453,10 @@ cudaError_t op_cut(pxr_handle* h) {
         k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
                                                h->act[h->acur ^ 1]);
     });
-    phase(h, kPhDisable, 1, [&] {
+    phase(h, kPhDisable, h->n_heavy ? 2 : 1, [&] {
         k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
+        if (h->n_heavy)
+            k_disable_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d, h->xt[h->xcur], nt);
     });
     phase(h, kPhCvol, 1, [&] { k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt); });
     phase(h, kPhBook, 1, [&] { k_round_end<OffT><<<1, 1, 0, s>>>(d); });
@@ -473,6 +497,7 @@ cudaError_t dispatch_w(pxr_handle* h, Op op, cudaGraphConditionalHandle cond) {
         default: return op_round<OffT, WV>(h);                   \
     }
     switch (h->W) {
+        case 1: PXR_OPS(1)
         case 4: PXR_OPS(4)
         case 16: PXR_OPS(16)
         case 32: PXR_OPS(32)
@@ -531,8 +556,11 @@ pxr_status build_loop_graph(pxr_handle* h, int key) {
     h->stream = h->own_stream;
     const bool prof = h->profiling;
     h->profiling = false;
+    const uint64_t launches_before = h->launches;
     e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     cudaError_t e2 = e == cudaSuccess ? dispatch(h, kOpLoopBody, cond) : e;
+    h->body_launches[key] = h->launches - launches_before;
+    h->launches = launches_before;   // counted when the graph runs
     cudaGraph_t captured = nullptr;
     if (e == cudaSuccess) e = cudaStreamEndCapture(h->stream, &captured);
     h->stream = user;
@@ -561,8 +589,13 @@ pxr_status decompose_graph(pxr_handle* h) {
     }
     k_loop_begin<<<1, 1, 0, h->stream>>>(h->ctr, h->cfg.max_rounds);
     PXR_CUDA(h, cudaGetLastError());
+    const uint32_t before = h->h_ctr->rounds;
     PXR_CUDA(h, cudaGraphLaunch(h->graphs[key], h->stream));
-    return sync_ctr(h);
+    pxr_status st = sync_ctr(h);
+    // the body (two rounds) ran ceil(rounds / 2) times, at least once
+    const uint32_t ran = h->h_ctr->rounds - before;
+    h->launches += 1 + h->body_launches[key] * std::max<uint64_t>(1, (ran + 1) / 2);
+    return st;
 }
 
 pxr_status decompose_stream(pxr_handle* h) {
@@ -620,7 +653,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->sort.pass_info, kMaxPasses + 1); A(&h->sort.tile_ctr, kMaxPasses); A(&h->sort.epoch, 1);
     A(&h->sort.status, (size_t)sort_tiles * kRadix);
     A(&h->sort_end_bit, 1); A(&h->root_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
-    A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 2);
+    A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 4); A(&h->heavy, N);
 #undef A
     if (e != cudaSuccess) { release(h); return cuda_fail(h, e, "cudaMalloc"); }
     h->sort.max_tiles = sort_tiles;
@@ -660,25 +693,29 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     h->xcur = h->tcur = h->acur = 0;
     PXR_CUDA(h, cudaMemcpyAsync(h->off, offsets, ((size_t)n + 1) * sizeof(OffT), kind, s));
     if (m) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, kind, s));
-    PXR_CUDA(h, cudaMemsetAsync(h->d_check, 0, 8, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->d_check, 0, 16, s));
     k_validate<OffT><<<grid_for(std::max<uint64_t>(h->slots, n)), kBlock, 0, s>>>(
-        static_cast<const OffT*>(h->off), h->cols, n, h->slots, &h->d_check[0], &h->d_check[1]);
+        static_cast<const OffT*>(h->off), h->cols, n, h->slots, &h->d_check[0], &h->d_check[1], h->heavy,
+        &h->d_check[2]);
     ++h->launches;
-    uint32_t check[2] = {0, 0};
-    PXR_CUDA(h, cudaMemcpyAsync(check, h->d_check, 8, cudaMemcpyDeviceToHost, s));
+    uint32_t check[4] = {0, 0, 0, 0};
+    PXR_CUDA(h, cudaMemcpyAsync(check, h->d_check, 16, cudaMemcpyDeviceToHost, s));
     PXR_CUDA(h, cudaStreamSynchronize(s));
     if (check[0] & 2u) return fail(h, PXR_INVALID_ARG, "offsets must start at 0 and end at 2m");
     if (check[0] & 1u) return fail(h, PXR_INVALID_ARG, "offsets must be non-decreasing");
     if (check[0] & 4u) return fail(h, PXR_INVALID_ARG, "column index out of range");
     h->maxdeg = check[1];
+    const uint32_t n_heavy = check[2];
     const uint32_t nb_bits = host_bitlen(std::max<uint64_t>(n, h->maxdeg));
-    // lanes per vertex: the power of two nearest the mean degree, 4..32
+    // lanes per vertex: one thread per row for sparse graphs (4 independent
+    // slots per step), more lanes as the mean degree grows
     const double mean = n ? (double)(2 * m) / n : 0.0;
-    const uint32_t W = mean <= 6.0 ? 4u : mean <= 12.0 ? 8u : mean <= 24.0 ? 16u : 32u;
+    const uint32_t W = mean <= 16.0 ? 1u : mean <= 32.0 ? 4u : mean <= 64.0 ? 8u : 32u;
     // captured round graphs bake in buffers, nb_bits and W: keep them only if all are unchanged
-    if (!reuse || nb_bits != h->nb_bits || W != h->W) drop_graphs(h);
+    if (!reuse || nb_bits != h->nb_bits || W != h->W || n_heavy != h->n_heavy) drop_graphs(h);
     h->nb_bits = nb_bits;
     h->W = W;
+    h->n_heavy = n_heavy;
     // round state: one cluster, every vertex active; keep the growing epochs
     RoundCtr c;
     PXR_CUDA(h, cudaMemcpyAsync(&c, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, s));

@@ -193,18 +193,25 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
     for (uint32_t j0 = warp0; j0 < count; j0 += groups) {
         const uint32_t j = j0 + (threadIdx.x & 31u) / W;
         const bool valid = j < count;
-        const uint32_t v = valid ? ids[j] : 0u;
-        const OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        uint32_t v = valid ? ids[j] : 0u;
+        OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
+        if (!light) beg = end;      // heavy rows: k_walk_heavy
         int64_t acc = 0;
-        for (OffT s = beg + gl; s < end; s += W) {
-            const uint32_t nb = d.cols[s];
-            ++st_s;
-            if (nb != kInvalidEdge) { acc += to_fixed(xt_in[nb], scale); ++st_g; }
+        for (OffT s = beg + gl; s < end; s += 4 * W) {
+            uint32_t nb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                st_s += s + u * W < end ? 1 : 0;
+                if (nb[u] != kInvalidEdge) { acc += to_fixed(xt_in[nb[u]], scale); ++st_g; }
+            }
         }
-        st_v += (valid && gl == 0) ? 1 : 0;
+        st_v += (light && gl == 0) ? 1 : 0;
 #pragma unroll
         for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o, W);
-        if (valid && gl == 0) {
+        if (light && gl == 0) {
             const double sum = __dmul_rn(__ll2double_rn(acc), inv);
             const double val = __dadd_rn(__dmul_rn(sum, 0.9), __dmul_rn((double)d.x[v], 0.1));
             const float xv = __double2float_rn(val);
@@ -247,18 +254,25 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
         const bool valid = j < count;
         const uint32_t v = valid ? ids[j] : 0u;
         const uint32_t mine = valid ? ordered_bits(d.x[v]) : 0u;
-        const OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
+        if (!light) beg = end;      // heavy rows: k_nodediff_heavy
         int32_t c = 0;
-        for (OffT s = beg + gl; s < end; s += W) {
-            const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge) continue;
-            const uint32_t o = ordered_bits(d.x[nb]);
-            const bool before = o < mine || (o == mine && nb < v);
-            c += before ? -1 : 1;
+        for (OffT s = beg + gl; s < end; s += 4 * W) {
+            uint32_t nb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (nb[u] == kInvalidEdge) continue;
+                const uint32_t o = ordered_bits(d.x[nb[u]]);
+                const bool before = o < mine || (o == mine && nb[u] < v);
+                c += before ? -1 : 1;
+            }
         }
 #pragma unroll
         for (int o = W / 2; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o, W);
-        if (valid && gl == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
+        if (light && gl == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
     }
 }
 
@@ -325,16 +339,9 @@ __global__ void __launch_bounds__(kBlock) k_sweep_scan(Dev<OffT> d, ClusterTable
     }
     uint64_t tile_total;
     const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
-    if (threadIdx.x == 0) {
-        if (tile == 0) {
-            lookback_publish(d.lb_scan, tile, epoch, 2u, tile_total);
-            s_excl = 0;
-        } else {
-            lookback_publish(d.lb_scan, tile, epoch, 1u, tile_total);
-            const uint64_t ex = lookback_exclusive<PairAdd>(d.lb_scan, tile, epoch, &d.ctr->err);
-            lookback_publish(d.lb_scan, tile, epoch, 2u, PairAdd::combine(ex, tile_total));
-            s_excl = ex;
-        }
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<PairAdd>(d.lb_scan, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
     }
     __syncthreads();
     // exclusive prefix of this thread = tile exclusive + (block inclusive - own run)
@@ -394,7 +401,8 @@ __global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTabl
         d.cut_off[c] = cut ? off : kNoCut;
         const bool split = cut || full;
         d.split[c] = split ? 1 : 0;
-        if (cut) atomicAdd(&d.ctr->n_cut, 1u);
+        const uint32_t cuts_in_warp = __ballot_sync(__activemask(), cut);
+        if (cut && (cuts_in_warp & lanemask_lt()) == 0u) atomicAdd(&d.ctr->n_cut, (uint32_t)__popc(cuts_in_warp));
         if (!split) {
             const uint32_t r = t.root[c];
             d.acc_max[r] = 0u;
@@ -434,18 +442,61 @@ __global__ void __launch_bounds__(kBlock) k_cut_init(Dev<OffT> d, ClusterTables 
     }
 }
 
+// Every parent pointer points to a smaller id (roots are hooked under smaller
+// roots), so a component's root is its minimum vertex and atomicMin can only
+// move a pointer closer to the root.  find() splits the path as it walks
+// with atomicMin, so a stored root is never replaced by a non-root ancestor.
 __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t v) {
     uint32_t p = ld_relaxed(&parent[v]);
     while (p != v) {
         const uint32_t gp = ld_relaxed(&parent[p]);
-        if (gp != p) {
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> r(parent[v]);
-            r.store(gp, cuda::memory_order_relaxed);  // path halving: gp is an ancestor of v
-        }
+        if (gp < p) atomicMin(&parent[v], gp);
         v = p;
         p = gp;
     }
     return v;
+}
+
+// First linking pass: each vertex of a split cluster points to its smallest
+// same-label neighbour below it (rows are sorted, so the first one found).
+// Only the owning thread writes parent[v] here.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
+                                                       const uint64_t* keys0, const uint64_t* keys1) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t sel = d.ctr->main_sel;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint64_t* keys = sel ? keys1 : keys0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(keys[j] >> 32);
+        if (!d.split[c]) continue;
+        const uint32_t v = vals[j];
+        const int32_t lv = d.lab[v];
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        for (OffT s = beg; s < end; ++s) {
+            const uint32_t nb = d.cols[s];
+            if (nb == kInvalidEdge) continue;  // disabled slots keep their place in the sorted row
+            if (nb >= v) break;                // no smaller neighbour left
+            if (d.lab[nb] == lv) { d.parent[v] = nb; break; }
+        }
+    }
+}
+
+// Flatten the linked forest: every vertex of a split cluster points at its root.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
+                                                     const uint64_t* keys0, const uint64_t* keys1) {
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t sel = d.ctr->main_sel;
+    const uint32_t* vals = sel ? vals1 : vals0;
+    const uint64_t* keys = sel ? keys1 : keys0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        const uint32_t c = (uint32_t)(keys[j] >> 32);
+        if (!d.split[c]) continue;
+        const uint32_t v = vals[j];
+        const uint32_t r = uf_find(d.parent, v);
+        atomicMin(&d.parent[v], r);
+    }
 }
 
 // union over same-label valid edges (ConsolidationManager::consolidate,
@@ -465,6 +516,7 @@ __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* v
         const uint32_t v = vals[j];
         const int32_t lv = d.lab[v];
         const OffT beg = d.off[v], end = d.off[v + 1];
+        if ((uint64_t)(end - beg) > kHeavyRow) continue;   // k_union_heavy
         for (OffT s = beg + gl; s < end; s += W) {
             const uint32_t nb = d.cols[s];
             if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
@@ -500,6 +552,8 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
         bool has = false, single = true;
         uint32_t k_first = 0, k_last = 0;
         ClusterAcc a_first = DataAgg::identity(), a_last = DataAgg::identity();
+        uint32_t my_roots[kScanItems];
+        uint32_t n_my = 0;
         for (int k = 0; k < kScanItems; ++k) {
             const uint32_t i = first + k;
             if (i >= count) break;
@@ -508,11 +562,11 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
             uint32_t r;
             if (d.split[c]) {
                 r = uf_find(d.parent, v);
-                cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(d.parent[v]).store(r, cuda::memory_order_relaxed);
-                if (r == v) roots[atomicAdd(&d.ctr->n_roots, 1u)] = r;
+                atomicMin(&d.parent[v], r);
+                if (r == v) my_roots[n_my++] = r;
             } else {
                 r = t.root[c];
-                if (i == t.start[c]) roots[atomicAdd(&d.ctr->n_roots, 1u)] = r;
+                if (i == t.start[c]) my_roots[n_my++] = r;
             }
             const float xv = d.x[v];
             const uint32_t ob = ordered_bits(xv);
@@ -529,6 +583,18 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
                 a_last = cur;
             }
         }
+        // register this warp's roots with one atomic
+        uint32_t incl = n_my;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if ((threadIdx.x & 31u) >= (uint32_t)o) incl += u;
+        }
+        const uint32_t warp_total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t slot = 0;
+        if ((threadIdx.x & 31u) == 31u && warp_total) slot = atomicAdd(&d.ctr->n_roots, warp_total);
+        slot = __shfl_sync(0xFFFFFFFFu, slot, 31) + incl - n_my;
+        for (uint32_t q = 0; q < n_my; ++q) roots[slot + q] = my_roots[q];
         emit_fragments<DataAgg>(has, single, k_first, a_first, k_last, a_last, agg);
     }
 }
@@ -572,17 +638,10 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
     }
     uint64_t tile_total;
     const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
-    if (threadIdx.x == 0) {
-        uint64_t ex = 0;
-        if (tile == 0) {
-            lookback_publish(d.lb_relabel, tile, epoch, 2u, tile_total);
-        } else {
-            lookback_publish(d.lb_relabel, tile, epoch, 1u, tile_total);
-            ex = lookback_exclusive<PairAdd>(d.lb_relabel, tile, epoch, &d.ctr->err);
-            lookback_publish(d.lb_relabel, tile, epoch, 2u, PairAdd::combine(ex, tile_total));
-        }
-        s_excl = ex;
-        if (tile == ntiles - 1) {
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<PairAdd>(d.lb_relabel, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
+        if (threadIdx.x == 0 && tile == ntiles - 1) {
             const uint64_t all = PairAdd::combine(ex, tile_total);
             d.ctr->n_keep = (uint32_t)all;
             d.ctr->n_active_next = (uint32_t)(all >> 32);
@@ -648,9 +707,9 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
         const uint32_t c = (uint32_t)(keys[i] >> 32);
         const uint32_t v = vals[i];
         vv[k] = v;
-        // find() again: a concurrent path-halving step in k_components_data may
-        // have replaced the stored root of v by a (non-root) ancestor
-        const uint32_t r = d.split[c] ? uf_find(d.parent, v) : t.root[c];
+        // k_components_data left parent[v] at the root (atomicMin stores only
+        // ever move a pointer towards the root)
+        const uint32_t r = d.split[c] ? d.parent[v] : t.root[c];
         const int32_t nl = d.newlab[r];
         d.lab[v] = nl;
         if (nl >= 0) {
@@ -661,16 +720,9 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
     }
     uint64_t tile_total;
     const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &tile_total);
-    if (threadIdx.x == 0) {
-        uint64_t ex = 0;
-        if (tile == 0) {
-            lookback_publish(d.lb_apply, tile, epoch, 2u, tile_total);
-        } else {
-            lookback_publish(d.lb_apply, tile, epoch, 1u, tile_total);
-            ex = lookback_exclusive<Add64>(d.lb_apply, tile, epoch, &d.ctr->err);
-            lookback_publish(d.lb_apply, tile, epoch, 2u, ex + tile_total);
-        }
-        s_excl = ex;
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(d.lb_apply, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
     }
     __syncthreads();
     uint32_t pos = (uint32_t)(s_excl + incl - run);
@@ -709,17 +761,12 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
     }
     uint64_t tile_total;
     const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &tile_total);
-    if (threadIdx.x == 0) {
-        uint64_t ex = 0;
-        if (tile == 0) {
-            lookback_publish(d.lb_ids, tile, epoch, 2u, tile_total);
-        } else {
-            lookback_publish(d.lb_ids, tile, epoch, 1u, tile_total);
-            ex = lookback_exclusive<Add64>(d.lb_ids, tile, epoch, &d.ctr->err);
-            lookback_publish(d.lb_ids, tile, epoch, 2u, ex + tile_total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(d.lb_ids, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) {
+            s_excl = ex;
+            s_n = (uint32_t)tile_total;
         }
-        s_excl = ex;
-        s_n = (uint32_t)tile_total;
     }
     __syncthreads();
     uint32_t lpos = (uint32_t)(incl - run);
@@ -744,17 +791,27 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         const bool valid = q < nkept;
         const uint32_t v = valid ? s_list[q] : 0u;
         const int32_t lv = valid ? d.lab[v] : 0;
-        const OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
+        const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
+        if (!light) beg = end;      // heavy rows: k_disable_heavy
         uint32_t deg = 0;
-        for (OffT s = beg + gl; s < end; s += W) {
-            const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge) continue;
-            if (d.lab[nb] != lv) d.cols[s] = kInvalidEdge;
-            else ++deg;
+        for (OffT s = beg + gl; s < end; s += 4 * W) {
+            uint32_t nb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            int32_t ln[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) ln[u] = nb[u] != kInvalidEdge ? d.lab[nb[u]] : lv;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (nb[u] == kInvalidEdge) continue;
+                if (ln[u] != lv) d.cols[s + u * W] = kInvalidEdge;
+                else ++deg;
+            }
         }
 #pragma unroll
         for (int o = W / 2; o > 0; o >>= 1) deg += __shfl_xor_sync(0xFFFFFFFFu, deg, o, W);
-        if (valid && gl == 0) {
+        if (light && gl == 0) {
             d.ideg[v] = deg;
             const float xv = d.x[v];
             xt[v] = deg ? __double2float_rn(__ddiv_rn((double)xv, (double)deg)) : 0.0f;
@@ -774,6 +831,141 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < kScanTile; q += kBlock)
         if (s_hkey[q] != 0xFFFFFFFFu && s_hval[q]) atomicAdd(&nt.vol[s_hkey[q]], s_hval[q]);
+}
+
+// ---------------------------------------------------------------------------
+// Heavy rows (> kHeavyRow slots): one CTA per vertex of the static heavy
+// list, kBlock threads over the row, block reduction.  Every accumulation is
+// order-independent, so the split between these and the lane-per-row kernels
+// does not change any result.
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kBlock / 32; ++w) t += sh[w];
+    return t;  // valid in thread 0
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_walk_heavy(Dev<OffT> d, const float* xt_in, float* xt_out) {
+    __shared__ int64_t sh[kBlock / 32];
+    __shared__ unsigned long long sh2[kBlock / 32];
+    const int e = fixed_exponent(d.ctr->xmax_bits, d.nb_bits);
+    const double scale = pow2(e), inv = pow2(-e);
+    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
+        const uint32_t v = d.heavy[h];
+        if (d.lab[v] < 0) continue;
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        int64_t acc = 0;
+        unsigned long long g = 0;
+        for (OffT s = beg + threadIdx.x; s < end; s += 4 * kBlock) {
+            uint32_t nb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * kBlock < end ? d.cols[s + u * kBlock] : kInvalidEdge;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (nb[u] != kInvalidEdge) { acc += to_fixed(xt_in[nb[u]], scale); ++g; }
+        }
+        acc = block_sum<int64_t>(acc, sh);
+        g = block_sum<unsigned long long>(g, sh2);
+        if (threadIdx.x == 0) {
+            const double sum = __dmul_rn(__ll2double_rn(acc), inv);
+            const double val = __dadd_rn(__dmul_rn(sum, 0.9), __dmul_rn((double)d.x[v], 0.1));
+            const float xv = __double2float_rn(val);
+            d.x[v] = xv;
+            const uint32_t dg = d.ideg[v];
+            xt_out[v] = dg ? __double2float_rn(__ddiv_rn((double)xv, (double)dg)) : 0.0f;
+            atomicMax(&d.ctr->xmax_walk_bits, __float_as_uint(fabsf(xv)));
+            atomicAdd(&d.ctr->stat_walk_vertices, 1ull);
+            atomicAdd(&d.ctr->stat_walk_slots, (unsigned long long)(end - beg));
+            atomicAdd(&d.ctr->stat_walk_gathers, g);
+        }
+    }
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_nodediff_heavy(Dev<OffT> d) {
+    __shared__ int32_t sh[kBlock / 32];
+    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
+        const uint32_t v = d.heavy[h];
+        if (d.lab[v] < 0) continue;
+        const uint32_t mine = ordered_bits(d.x[v]);
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        int32_t c = 0;
+        for (OffT s = beg + threadIdx.x; s < end; s += 4 * kBlock) {
+            uint32_t nb[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * kBlock < end ? d.cols[s + u * kBlock] : kInvalidEdge;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (nb[u] == kInvalidEdge) continue;
+                const uint32_t o = ordered_bits(d.x[nb[u]]);
+                c += (o < mine || (o == mine && nb[u] < v)) ? -1 : 1;
+            }
+        }
+        c = block_sum<int32_t>(c, sh);
+        if (threadIdx.x == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
+    }
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_union_heavy(Dev<OffT> d) {
+    const uint32_t k = d.ctr->n_clusters;
+    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
+        const uint32_t v = d.heavy[h];
+        const int32_t lv = d.lab[v];
+        if (lv < 0) continue;
+        const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;   // cut labels are c or K + c
+        if (c >= k || !d.split[c]) continue;
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        for (OffT s = beg + threadIdx.x; s < end; s += kBlock) {
+            const uint32_t nb = d.cols[s];
+            if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
+            uint32_t a = v, b = nb;
+            for (uint32_t tries = 0;; ++tries) {
+                if (tries > kSpinLimit) { atomicOr(&d.ctr->err, kErrUnionFind); break; }
+                const uint32_t ra = uf_find(d.parent, a), rb = uf_find(d.parent, b);
+                if (ra == rb) break;
+                const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+                if (atomicCAS(&d.parent[hi], hi, lo) == hi) break;
+                a = hi;
+                b = lo;
+            }
+        }
+    }
+}
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_disable_heavy(Dev<OffT> d, float* xt, ClusterTables nt) {
+    __shared__ uint32_t sh[kBlock / 32];
+    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
+        const uint32_t v = d.heavy[h];
+        const int32_t lv = d.lab[v];
+        if (lv < 0) continue;
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        uint32_t deg = 0;
+        for (OffT s = beg + threadIdx.x; s < end; s += kBlock) {
+            const uint32_t nb = d.cols[s];
+            if (nb == kInvalidEdge) continue;
+            if (d.lab[nb] != lv) d.cols[s] = kInvalidEdge;
+            else ++deg;
+        }
+        deg = block_sum<uint32_t>(deg, sh);
+        if (threadIdx.x == 0) {
+            d.ideg[v] = deg;
+            const float xv = d.x[v];
+            xt[v] = deg ? __double2float_rn(__ddiv_rn((double)xv, (double)deg)) : 0.0f;
+            atomicMax(&d.ctr->xmax_bits, __float_as_uint(fabsf(xv)));
+            atomicAdd(&nt.vol[lv], deg);
+        }
+    }
 }
 
 // exclusive prefix of cluster volumes over labels
@@ -797,16 +989,9 @@ __global__ void __launch_bounds__(kBlock) k_cvol_scan(Dev<OffT> d, ClusterTables
     }
     uint64_t tile_total;
     const uint64_t incl = block_inclusive<Add64>(run, warp_tot, &tile_total);
-    if (threadIdx.x == 0) {
-        uint64_t ex = 0;
-        if (tile == 0) {
-            lookback_publish(d.lb_cvol, tile, epoch, 2u, tile_total);
-        } else {
-            lookback_publish(d.lb_cvol, tile, epoch, 1u, tile_total);
-            ex = lookback_exclusive<Add64>(d.lb_cvol, tile, epoch, &d.ctr->err);
-            lookback_publish(d.lb_cvol, tile, epoch, 2u, ex + tile_total);
-        }
-        s_excl = ex;
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(d.lb_cvol, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
     }
     __syncthreads();
     uint64_t p = s_excl + incl - run;

@@ -73,7 +73,13 @@ struct Dev {
     SortState sort;
     uint32_t* sort_end_bit;   // main sort bits
     uint32_t* root_end_bit;   // root sort bits
+    const uint32_t* heavy;    // vertices whose row exceeds kHeavyRow slots (one CTA each)
+    uint32_t n_heavy;
 };
+
+// Rows longer than this are processed by a whole CTA in the *_heavy kernels
+// and skipped by the lane-per-row kernels.
+constexpr uint32_t kHeavyRow = 64;
 
 // look-back sites (index into Dev::lb_epoch and RoundCtr::tile_counter)
 enum : int { kSiteScan = 0, kSiteRelabel = 1, kSiteApply = 2, kSiteIds = 3, kSiteCvol = 4 };

@@ -20,7 +20,10 @@
 namespace pxr {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
+#ifndef PXR_SORT_ITEMS
+#define PXR_SORT_ITEMS 16
+#endif
+constexpr int kSortItems = PXR_SORT_ITEMS;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;
@@ -107,7 +110,10 @@ __device__ __forceinline__ uint64_t sort_status_word(uint32_t epoch, uint32_t fl
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortBuffers<K> b, SortState s, int pass,
+#ifndef PXR_SORT_MIN_BLOCKS
+#define PXR_SORT_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_kernel(SortBuffers<K> b, SortState s, int pass,
                                                                  uint32_t* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K* skeys = reinterpret_cast<K*>(smem_raw);

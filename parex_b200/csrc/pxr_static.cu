@@ -102,18 +102,11 @@ __global__ void __launch_bounds__(kBlock) k_static_rank(unsigned char* base, int
     }
     uint64_t total;
     const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &total);
-    if (threadIdx.x == 0) {
-        uint64_t ex = 0;
-        if (tile == 0) {
-            lookback_publish(lb, tile, epoch, 2u, total);
-        } else {
-            lookback_publish(lb, tile, epoch, 1u, total);
-            ex = lookback_exclusive<Add64>(lb, tile, epoch, &ctr->err);
-            lookback_publish(lb, tile, epoch, 2u, ex + total);
-        }
-        s_excl = ex;
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(lb, tile, epoch, total, &ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
         // a device-side wait that ran out (sort or look-back) is reported as -1
-        if (tile == ntiles - 1) *num_out = ctr->err ? -1 : (int32_t)(ex + total);
+        if (threadIdx.x == 0 && tile == ntiles - 1) *num_out = ctr->err ? -1 : (int32_t)(ex + total);
     }
     __syncthreads();
     uint32_t r = (uint32_t)(s_excl + incl - run);
