@@ -273,24 +273,32 @@ def product_arm(args, rank, world, local_rank):
     h2d = (n + 1) * 4 + 2 * m * 4
     d2h = n * 4 + 4
 
-    # roofline of the dominant phase among those with algorithmic byte counts
+    # roofline of the dominant phase among those with algorithmic byte counts;
+    # per launch: the sort counts its active digit passes, the walk one launch per round
     peak, peak_kind = measured_peaks()
     by = {p["name"]: p for p in phases}
     walk_bytes = 28 * pst["walk_vertices"] + 4 * pst["walk_slots"] + 4 * pst["walk_gathers"]
     sort_bytes = 24 * pst["sort_items"]
-    cands = {"walk": walk_bytes, "sort": sort_bytes}
+    cands = {"walk": (walk_bytes, max(1, pst["rounds"])), "sort": (sort_bytes, max(1, pst["sort_passes"]))}
     dom = max(cands, key=lambda k: by[k]["ms"])
-    ach = cands[dom] / (by[dom]["ms"] / 1e3) / 1e9
+    alg_total, units = cands[dom]
+    ach = alg_total / (by[dom]["ms"] / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(dom)
+            tj = json.load(f)
+        if dom == "sort" and "sort" in tj:
+            traffic = tj["sort"]["dram_bytes_per_item_pass"] * pst["sort_items"] / units
+        elif dom == "walk" and "walk" in tj:
+            traffic = tj["walk"]["dram_over_algorithmic"] * alg_total / units
     total_phase = sum(p["ms"] for p in phases)
     roofline = {
         "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
-        "kernel": {"walk": "k_walk", "sort": "sort_pass_kernel (+histogram, plan)"}[dom],
-        "algorithmic_bytes": cands[dom], "device_ms": by[dom]["ms"], "launches": by[dom]["launches"],
+        "kernel": {"walk": "k_walk", "sort": "sort_pass_kernel<u64> (time includes histogram, plan)"}[dom],
+        "algorithmic_bytes_per_launch": alg_total / units, "launches": units,
+        "device_ms": by[dom]["ms"], "device_us_per_launch": 1e3 * by[dom]["ms"] / units,
+        "traffic_source": "profiles/traffic.json: ncu DRAM bytes of full-size round-1 launches, scaled by items",
         "peak_source": f"{peak_kind} HBM copy peak",
         "phase_share": {p["name"]: round(p["ms"] / total_phase, 4) for p in phases if p["ms"] > 0},
         "prof_run_identical": prof_labels_equal,

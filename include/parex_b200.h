@@ -81,6 +81,7 @@ typedef struct {
     uint64_t walk_slots;         /* CSR slots read by walk steps since initialization      */
     uint64_t walk_gathers;       /* valid-neighbour gathers by walk steps                  */
     uint64_t sort_items;         /* items x passes moved by the sweep sort                 */
+    uint64_t sort_passes;        /* digit passes the sweep sort ran (constant digits skip)  */
 } pxr_stats;
 
 /* Per-phase device time, recorded with CUDA events when profiling is on

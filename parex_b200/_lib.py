@@ -52,7 +52,7 @@ class Stats(C.Structure):
                 ("clusters_with_cut", C.c_uint32), ("device_bytes", C.c_uint64),
                 ("last_decompose_ms", C.c_double), ("kernel_launches", C.c_uint64),
                 ("walk_vertices", C.c_uint64), ("walk_slots", C.c_uint64), ("walk_gathers", C.c_uint64),
-                ("sort_items", C.c_uint64)]
+                ("sort_items", C.c_uint64), ("sort_passes", C.c_uint64)]
 
 
 class PhaseStat(C.Structure):

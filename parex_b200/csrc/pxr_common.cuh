@@ -48,6 +48,7 @@ struct RoundCtr {
     unsigned long long stat_walk_slots;
     unsigned long long stat_walk_gathers;
     unsigned long long stat_sort_items;
+    unsigned long long stat_sort_passes;
 };
 
 // ---------------------------------------------------------------------------

@@ -1055,6 +1055,7 @@ pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out) {
     out->walk_slots = h->h_ctr->stat_walk_slots;
     out->walk_gathers = h->h_ctr->stat_walk_gathers;
     out->sort_items = h->h_ctr->stat_sort_items;
+    out->sort_passes = h->h_ctr->stat_sort_passes;
     return st;
 }
 

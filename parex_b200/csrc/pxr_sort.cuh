@@ -36,7 +36,7 @@ struct SortState {
     uint32_t* epoch;      // [1]
     uint64_t* status;     // [max_tiles][kRadix]
     uint32_t max_tiles;
-    unsigned long long* items_moved;  // optional: += items x active passes
+    unsigned long long* items_moved;  // optional: [0] += items x active passes, [1] += active passes
 };
 
 template <typename K>
@@ -101,7 +101,10 @@ __global__ void __launch_bounds__(kRadix) sort_plan_kernel(SortBuffers<K> b, Sor
         *s.epoch = *s.epoch + kMaxPasses;
         uint32_t active = 0;
         for (int p = 0; p < kMaxPasses; ++p) active += s.pass_info[p] & 1u;
-        if (s.items_moved) *s.items_moved += (unsigned long long)count * active;
+        if (s.items_moved) {
+            s.items_moved[0] += (unsigned long long)count * active;
+            s.items_moved[1] += active;
+        }
     }
 }
 
