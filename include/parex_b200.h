@@ -111,7 +111,9 @@ pxr_status pxr_set_stream(pxr_handle* h, void* stream);
 /* CudaDeviceManager::initialize(const Graph&) (cuda/interface.h:24;
  * cuda/device.h:86-100).  Uploads the CSR (n+1 offsets, 2m columns), resets
  * the partition to one cluster and seeds the potentials from cfg.seed.
- * Offsets are 32-bit (the reference's EdgeIx) or 64-bit. */
+ * Offsets are 32-bit (the reference's EdgeIx) or 64-bit; the starting
+ * cluster's volume 2m must be below 2^32 (32-bit prefix volumes, as the
+ * reference's NodeData). */
 pxr_status pxr_initialize(pxr_handle* h, uint32_t n, uint64_t m,
                           const uint32_t* offsets, const uint32_t* cols);
 pxr_status pxr_initialize64(pxr_handle* h, uint32_t n, uint64_t m,
@@ -123,6 +125,22 @@ pxr_status pxr_initialize64(pxr_handle* h, uint32_t n, uint64_t m,
 pxr_status pxr_initialize_device(pxr_handle* h, uint32_t n, uint64_t m,
                                  const void* offsets, int offsets_are_64bit,
                                  const uint32_t* cols);
+
+/* Batched independent instances.  No counterpart in the reference, which
+ * decomposes one graph per CudaDeviceManager.  The CSR (host arrays, 64-bit
+ * offsets) is the disjoint union of n_instances graphs; instance i owns the
+ * vertices [instance_start[i], instance_start[i+1]) (instance_start has
+ * n_instances + 1 entries, runs from 0 to n, every instance non-empty) and no
+ * edge may join two instances (PXR_INVALID_ARG otherwise).  Every instance
+ * starts as its own cluster, so the whole batch, from a handful of vertices
+ * to millions per instance, advances through the same rounds: one walk
+ * launch, one sort, one scan and one components pass per round for all of
+ * them.  The volume of each instance must be below 2^32 (the reference's
+ * 32-bit prefix volumes); the batch as a whole may exceed it.  Potentials are
+ * seeded as pxr_initialize does, by global vertex id. */
+pxr_status pxr_initialize_batched(pxr_handle* h, uint32_t n, uint64_t m,
+                                  const uint64_t* offsets, const uint32_t* cols,
+                                  uint32_t n_instances, const uint32_t* instance_start);
 
 /* CudaDeviceManager::iterateRandomWalk() (cuda/interface.h:29). */
 pxr_status pxr_walk_step(pxr_handle* h);

@@ -27,7 +27,7 @@ SYMBOLS = [
     "pxr_download_partition", "pxr_final_partition", "pxr_num_cut_edges", "pxr_download_graph",
     "pxr_download_graph64", "pxr_download_degrees", "pxr_download_labels", "pxr_active_edge_map",
     "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
-    "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state",
+    "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -111,6 +111,7 @@ def load() -> C.CDLL:
     L.pxr_final_partition_static.argtypes = [p, u32, p, p, p]
     L.pxr_set_potentials.argtypes = [p, p]
     L.pxr_set_state.argtypes = [p, p, p, u32, p, p, p, u32, i32, C.c_int]
+    L.pxr_initialize_batched.argtypes = [p, u32, u64, p, p, u32, p]
     for name in SYMBOLS:
         fn = getattr(L, name)
         if name not in ("pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_destroy"):

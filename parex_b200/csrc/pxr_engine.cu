@@ -86,6 +86,46 @@ __global__ void k_degrees(const OffT* off, uint32_t n, uint32_t* ideg, int32_t* 
     }
 }
 
+// Batched instances: label = index of the instance that owns the vertex
+// (binary search of the instance starts), the instance volumes, and a flag
+// when an edge leaves its instance.
+template <typename OffT>
+__global__ void k_batch_setup(const OffT* off, const uint32_t* cols, const uint32_t* ideg, const uint32_t* starts,
+                              uint32_t n, uint32_t n_inst, int32_t* lab, unsigned long long* vol, uint32_t* bad) {
+    for (uint32_t v0 = blockIdx.x * blockDim.x; v0 < n; v0 += gridDim.x * blockDim.x) {
+        const uint32_t v = v0 + threadIdx.x;
+        const bool valid = v < n;
+        uint32_t inst = 0;
+        if (valid) {
+            uint32_t lo = 0, hi = n_inst;   // starts[0] = 0 <= v < starts[n_inst] = n
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (starts[mid] <= v) lo = mid; else hi = mid;
+            }
+            inst = lo;
+            lab[v] = (int32_t)inst;
+            const uint32_t a = starts[inst], b = starts[inst + 1];
+            bool out = false;
+            for (OffT e = off[v]; e < off[v + 1]; ++e) {
+                const uint32_t u = cols[e];
+                out |= u != kInvalidEdge && (u < a || u >= b);
+            }
+            if (out) atomicOr(bad, 1u);
+        }
+        // one atomic per warp when the whole warp lies in one instance
+        const unsigned long long dg = valid ? ideg[v] : 0ull;
+        const uint32_t first = __shfl_sync(0xFFFFFFFFu, inst, 0);
+        if (__all_sync(0xFFFFFFFFu, !valid || inst == first)) {
+            unsigned long long sum = dg;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+            if ((threadIdx.x & 31u) == 0 && sum) atomicAdd(&vol[first], sum);
+        } else if (valid && dg) {
+            atomicAdd(&vol[inst], dg);
+        }
+    }
+}
+
 // x~ = x / internal degree for every vertex, and max |x| over every vertex
 __global__ void k_refresh_scaled(const float* x, const uint32_t* ideg, uint32_t n, float* xt, uint32_t* xmax_bits) {
     uint32_t vmax = 0;
@@ -678,10 +718,13 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
 // offsets/cols: host pointers (kind = cudaMemcpyHostToDevice) or device pointers
 template <typename OffT>
 pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* offsets, const uint32_t* cols,
-                           cudaMemcpyKind kind) {
+                           cudaMemcpyKind kind, bool batched = false) {
     if (!h) return PXR_INVALID_ARG;
     if (!offsets || (m > 0 && !cols)) return fail(h, PXR_INVALID_ARG, "null graph pointer");
     if (n >= 0x7FFFFFFFu) return fail(h, PXR_INVALID_ARG, "n must be below 2^31 - 1");
+    // cluster volumes are 32-bit (NodeData::prefix_volume, lib/core/definitions.h)
+    if (!batched && 2 * m >= (1ull << 32))
+        return fail(h, PXR_INVALID_ARG, "the volume 2m of the starting cluster must be below 2^32");
     PXR_CUDA(h, cudaSetDevice(h->device));
     h->initialized = false;
     const bool reuse = !h->allocs.empty() && h->n == n && h->m == m && h->off64 == (sizeof(OffT) == 8);
@@ -739,6 +782,58 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     pxr_status st = setup_tables_initial(h);
     if (st != PXR_OK) return st;
     PXR_CUDA(h, cudaGetLastError());
+    if (batched) return PXR_OK;   // batch_setup completes the state
+    h->initialized = true;
+    return sync_ctr(h);
+}
+
+// Every instance becomes its own cluster: labels, cluster tables and the
+// round counters replace the one-cluster state that initialize_impl left.
+template <typename OffT>
+pxr_status batch_setup(pxr_handle* h, uint32_t n_inst, const uint32_t* starts) {
+    const uint32_t n = h->n;
+    cudaStream_t s = h->stream;
+    uint32_t* d_starts = nullptr;
+    unsigned long long* d_vol = nullptr;
+    cudaError_t e = cudaMalloc(&d_starts, ((size_t)n_inst + 1) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&d_vol, (size_t)n_inst * 8);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_starts, starts, ((size_t)n_inst + 1) * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_vol, 0, (size_t)n_inst * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&h->d_check[3], 0, 4, s);
+    if (e == cudaSuccess) {
+        k_batch_setup<OffT><<<grid_for(n), kBlock, 0, s>>>(static_cast<const OffT*>(h->off), h->cols, h->ideg, d_starts,
+                                                           n, n_inst, h->lab, d_vol, &h->d_check[3]);
+        ++h->launches;
+        e = cudaGetLastError();
+    }
+    std::vector<unsigned long long> vol(n_inst);
+    uint32_t bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vol.data(), d_vol, (size_t)n_inst * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, &h->d_check[3], 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_starts);
+    cudaFree(d_vol);
+    if (e != cudaSuccess) return cuda_fail(h, e, "batched set-up");
+    if (bad) return fail(h, PXR_INVALID_ARG, "an edge joins two instances");
+    std::vector<uint32_t> start(n_inst), size(n_inst), vol32(n_inst), vol_start(n_inst), root(n_inst);
+    uint64_t acc = 0;
+    for (uint32_t i = 0; i < n_inst; ++i) {
+        if (vol[i] >= (1ull << 32)) return fail(h, PXR_INVALID_ARG, "instance volume must be below 2^32");
+        start[i] = starts[i];
+        size[i] = starts[i + 1] - starts[i];
+        root[i] = starts[i];
+        vol32[i] = (uint32_t)vol[i];
+        vol_start[i] = (uint32_t)acc;   // prefixes are used modulo 2^32, per cluster
+        acc += vol[i];
+    }
+    const ClusterTables& t = h->tab[h->tcur];
+    PXR_CUDA(h, cudaMemcpyAsync(t.start, start.data(), n_inst * 4ull, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(t.size, size.data(), n_inst * 4ull, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(t.vol, vol32.data(), n_inst * 4ull, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(t.vol_start, vol_start.data(), n_inst * 4ull, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(t.root, root.data(), n_inst * 4ull, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemsetAsync(t.best, 0xFF, n_inst * 8ull, s));
+    PXR_CUDA(h, cudaMemcpyAsync(&h->ctr->n_clusters, &n_inst, 4, cudaMemcpyHostToDevice, s));
     h->initialized = true;
     return sync_ctr(h);
 }
@@ -850,6 +945,28 @@ pxr_status pxr_initialize_device(pxr_handle* h, uint32_t n, uint64_t m, const vo
         return initialize_impl<uint64_t>(h, n, m, static_cast<const uint64_t*>(offsets), cols, cudaMemcpyDeviceToDevice);
     if (2 * m >= (1ull << 32)) return fail(h, PXR_INVALID_ARG, "32-bit offsets need 2m < 2^32");
     return initialize_impl<uint32_t>(h, n, m, static_cast<const uint32_t*>(offsets), cols, cudaMemcpyDeviceToDevice);
+}
+
+pxr_status pxr_initialize_batched(pxr_handle* h, uint32_t n, uint64_t m, const uint64_t* offsets, const uint32_t* cols,
+                                  uint32_t n_instances, const uint32_t* instance_start) {
+    if (!h) return PXR_INVALID_ARG;
+    if (!instance_start || n_instances == 0) return fail(h, PXR_INVALID_ARG, "no instances");
+    if (instance_start[0] != 0 || instance_start[n_instances] != n)
+        return fail(h, PXR_INVALID_ARG, "instance starts must run from 0 to n");
+    for (uint32_t i = 0; i < n_instances; ++i)
+        if (instance_start[i + 1] <= instance_start[i])
+            return fail(h, PXR_INVALID_ARG, "every instance needs at least one vertex");
+    pxr_status st;
+    if (offsets && 2 * m < (1ull << 32)) {
+        std::vector<uint32_t> o32((size_t)n + 1);
+        for (size_t i = 0; i <= n; ++i) o32[i] = (uint32_t)offsets[i];
+        st = initialize_impl<uint32_t>(h, n, m, o32.data(), cols, cudaMemcpyHostToDevice, true);
+        if (st != PXR_OK) return st;
+        return batch_setup<uint32_t>(h, n_instances, instance_start);
+    }
+    st = initialize_impl<uint64_t>(h, n, m, offsets, cols, cudaMemcpyHostToDevice, true);
+    if (st != PXR_OK) return st;
+    return batch_setup<uint64_t>(h, n_instances, instance_start);
 }
 
 pxr_status pxr_walk_step(pxr_handle* h) { return run_op(h, kOpWalk); }

@@ -109,6 +109,23 @@ class CudaDeviceManager:
             self._call(self._L.pxr_initialize, n, m, _ptr(off), _ptr(cols))
         self.n, self.m = n, m
 
+    def initialize_batched(self, graph, instance_start) -> None:
+        """Disjoint union of independent instances, each its own starting
+        cluster (pxr_initialize_batched); ``instance_start`` has one entry per
+        instance plus the final n."""
+        if isinstance(graph, CSRGraph):
+            offsets, cols = graph.offsets, graph.cols
+        else:
+            offsets, cols = graph
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        starts = np.ascontiguousarray(instance_start, dtype=np.uint32)
+        n = int(off.shape[0] - 1)
+        m = int(cols.shape[0] // 2)
+        self._call(self._L.pxr_initialize_batched, n, m, _ptr(off), _ptr(cols), int(starts.shape[0] - 1),
+                   _ptr(starts))
+        self.n, self.m = n, m
+
     def iterateRandomWalk(self) -> None:
         self._call(self._L.pxr_walk_step)
 
