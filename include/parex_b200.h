@@ -82,6 +82,9 @@ typedef struct {
     uint64_t walk_gathers;       /* valid-neighbour gathers by walk steps                  */
     uint64_t sort_items;         /* items x passes moved by the sweep sort                 */
     uint64_t sort_passes;        /* digit passes the sweep sort ran (constant digits skip)  */
+    uint64_t swept_items;        /* sweep input vertices summed over rounds                */
+    uint64_t skipped_sweeps;     /* cluster-rounds the learned schedule did not sweep      */
+    uint64_t false_stops;        /* skipped sweeps that would have cut (audit mode only)    */
 } pxr_stats;
 
 /* Per-phase device time, recorded with CUDA events when profiling is on
@@ -91,6 +94,61 @@ typedef struct {
     double ms;                   /* summed device time                                    */
     uint64_t launches;           /* kernel launches in this phase                         */
 } pxr_phase_stat;
+
+/* ---- learned sweep schedule (no counterpart in the reference) -------------
+ *
+ * The reference sweeps every active cluster in every round.  The learned
+ * schedule lets a cluster skip the sweep (sort, scan, cut, components,
+ * recentering) for a number of rounds predicted by a small MLP from the
+ * cluster's features; its vertices keep walking.  The MLP never decides a cut
+ * or a certificate: cuts are chosen and scored by the exact sweep when the
+ * cluster is next swept, and a cluster is certified only by the plain check
+ * (potential spread below rw_threshold, or fewer than 2 vertices).
+ * Network: 16 features -> 32 -> 32 -> 1 (ReLU), bf16 weights and inputs,
+ * float accumulation; output y = predicted log2(1 + rounds the cluster can
+ * skip); the schedule skips floor(safety * (2^y - 1)) rounds, at most
+ * max_skip.  Parameter layout (PXR_MLP_PARAMS bf16 values): W1[32][16], b1[32],
+ * W2[32][32], b2[32], W3[32], b3.  norm: 16 input means then 16 scales;
+ * the MLP reads bf16((feature - mean) * scale). */
+#define PXR_MLP_FEATURES 16
+#define PXR_MLP_HIDDEN 32
+#define PXR_MLP_PARAMS 1633
+
+enum {
+    PXR_SCHEDULE_PLAIN = 0,    /* every active cluster swept every round (the reference's method)  */
+    PXR_SCHEDULE_LEARNED = 1,  /* clusters skip the sweep for the rounds the MLP predicts           */
+    PXR_SCHEDULE_AUDIT = 2     /* as LEARNED, but skipped clusters are still swept (not acted on)
+                                  and those whose sweep would have cut are counted (false_stops);
+                                  the partition is the same as with LEARNED                          */
+};
+
+typedef struct {
+    uint32_t mode;             /* PXR_SCHEDULE_*                                                    */
+    uint32_t trace;            /* nonzero: keep one pxr_cluster_record per active cluster per round */
+    float safety;              /* fraction of the predicted skips taken                             */
+    uint32_t max_skip;         /* cap on consecutive skipped rounds                                 */
+    uint32_t reserved[4];
+} pxr_schedule;
+
+/* One active cluster after the last round (trace mode).  origin: 1 swept and
+ * not split, 2 new from a split (swept next round), 3 carried unswept. */
+typedef struct {
+    uint32_t root, size, volume, origin;
+    float potential;           /* max - min of the potentials at this round's sweep              */
+    float sparsity;            /* best sweep sparsity of this round (of the parent for origin 2) */
+    float prev_potential, prev_sparsity;
+    uint32_t prev_round;       /* round of the previous sweep of the same vertex set             */
+    uint32_t age;              /* earlier sweeps of the same vertex set                          */
+    uint32_t round;            /* rounds completed before this one                                */
+    uint32_t skip;             /* rounds the schedule carries the cluster next                    */
+    float prediction;          /* MLP output y (learned modes)                                    */
+    uint32_t has_prev;
+    uint32_t reserved[2];
+    float features[PXR_MLP_FEATURES];
+} pxr_cluster_record;
+
+typedef struct { float delta; float over_weight; } pxr_mlp_loss;       /* asymmetric Huber */
+typedef struct { float lr, beta1, beta2, eps; } pxr_mlp_adam;
 
 void pxr_config_default(pxr_config* cfg);
 const char* pxr_status_string(pxr_status s);
@@ -224,6 +282,31 @@ pxr_status pxr_set_potentials(pxr_handle* h, const double* x);
 pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* act, uint32_t n_act,
                          const double* x, const uint32_t* internal_degrees, const uint32_t* cols,
                          uint32_t n_clusters, int32_t smallest_label, int full_components);
+
+/* Learned sweep schedule: mode, trace and, for the learned modes, the MLP
+ * (weights: PXR_MLP_PARAMS bf16 bit patterns, norm: 32 floats; host memory).
+ * Takes effect from the next round; every cluster is due at (re)initialisation. */
+pxr_status pxr_set_schedule(pxr_handle* h, const pxr_schedule* cfg, const uint16_t* weights, const float* norm);
+/* Records of the active clusters after the last round (trace mode): writes
+ * min(cap, count) and sets *count. */
+pxr_status pxr_read_cluster_records(pxr_handle* h, pxr_cluster_record* out, uint32_t cap, uint32_t* count);
+
+/* MLP kernels on device arrays (the caller's stream; NULL = legacy stream).
+ * features: n x 16 floats; weights: PXR_MLP_PARAMS bf16; norm: 32 floats. */
+pxr_status pxr_mlp_forward(const float* features, uint32_t n, const uint16_t* weights, const float* norm,
+                           float* out, void* stream);
+/* Floats of scratch pxr_mlp_gradient needs for n samples. */
+size_t pxr_mlp_scratch_floats(uint32_t n);
+/* Mean loss and its gradient over n samples (targets: n floats): asymmetric
+ * Huber on e = y - target, weight over_weight when e > 0, quadratic for
+ * |e| <= delta.  grad: PXR_MLP_PARAMS floats; loss_out: 1 float. */
+pxr_status pxr_mlp_gradient(const float* features, const float* targets, uint32_t n, const uint16_t* weights,
+                            const float* norm, const pxr_mlp_loss* loss, float* scratch, float* grad,
+                            float* loss_out, void* stream);
+/* One Adam step on float master weights (m, v: moments; step counts from 1),
+ * then weights = bf16(master). */
+pxr_status pxr_mlp_adam_step(float* master, float* m, float* v, const float* grad, uint16_t* weights,
+                             uint32_t step, const pxr_mlp_adam* opt, void* stream);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,7 @@ def lib():
                      "orc_cluster_data_stage", "orc_recenter_stage", "orc_disable_stage",
                      "orc_cut_clusters", "orc_rekey"]:
             getattr(L, name).argtypes = [p]
+        L.orc_scheduled_round.argtypes = [p, p]
         L.orc_decompose.argtypes = [p, C.c_uint32]
         L.orc_decompose.restype = C.c_uint32
         L.orc_final_partition.argtypes = [p, p]
@@ -136,6 +137,12 @@ class Oracle:
     def disable_stage(self): lib().orc_disable_stage(self._s)
     def cut_clusters(self): lib().orc_cut_clusters(self._s)
     def rekey(self): lib().orc_rekey(self._s)
+
+    def scheduled_round(self, due) -> None:
+        """One round in which only the clusters with due[c] != 0 are swept."""
+        due = np.ascontiguousarray(due, dtype=np.uint8)
+        assert due.shape[0] >= self.n_clusters
+        lib().orc_scheduled_round(self._s, _ptr(due) if due.size else None)
 
     def decompose(self, max_rounds: int = 200000) -> int:
         return int(lib().orc_decompose(self._s, max_rounds))

@@ -615,6 +615,127 @@ void orc_cut_clusters(orc_state* s) {
     orc_disable_stage(s);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Scheduled round (no reference counterpart: the sweep schedule of the
+ * learned stop predictor).  Every active vertex walks; only the clusters with
+ * due[c] != 0 go through the sweep, the cut, components, cluster data,
+ * recentering and edge disabling, exactly as in the plain round.  The other
+ * ("carried") clusters keep their vertices, potentials and rows; they are
+ * relabelled with the rest: dense labels in the order of the clusters' root
+ * vertices (minimum vertex id) over swept and carried clusters together, and
+ * a swept cluster that is certified takes smallest - j - 1 with j its position
+ * in that merged root order.  smallest is the least label of the sweep (0 when
+ * it holds no negative label).  With every cluster due this is the plain
+ * round. */
+
+static const uint32_t* g_root_of;
+static int cmp_root_entry(const void* a, const void* b) {
+    const uint32_t ra = g_root_of[*(const uint32_t*)a], rb = g_root_of[*(const uint32_t*)b];
+    return ra < rb ? -1 : (ra > rb);
+}
+
+void orc_scheduled_round(orc_state* s, const uint8_t* due) {
+    const uint32_t K = s->n_clusters;
+    orc_walk(s);
+    const uint32_t nA = s->n_act;
+    orc_lnode* carried = (orc_lnode*)xcalloc(nA ? nA : 1, sizeof(orc_lnode));
+    uint32_t* croot = (uint32_t*)xcalloc(K ? K : 1, 4);
+    for (uint32_t c = 0; c < K; ++c) croot[c] = 0xFFFFFFFFu;
+    uint32_t nd = 0, nc = 0;
+    for (uint32_t i = 0; i < nA; ++i) {
+        const orc_lnode a = s->act[i];
+        if (a.label < 0 || due[a.label]) {
+            s->act[nd] = a;
+            s->keys[nd] = s->keys[i];
+            ++nd;
+        } else {
+            carried[nc++] = a;
+            if (a.nix < croot[a.label]) croot[a.label] = a.nix;
+        }
+    }
+    s->n_act = nd;
+    if (nd > 0) {
+        orc_sweep(s);
+        if (s->smallest > 0) s->smallest = 0;
+    } else {
+        s->smallest = 0;
+        s->k_sweep = 0;
+        s->n_cut = 0;
+        s->n_clusters = 0;
+    }
+    orc_cut_stage(s);
+    orc_components_stage(s);
+    orc_cluster_data_stage(s);
+
+    /* merged root order: swept clusters (cluster data) and carried clusters */
+    const uint32_t kd = s->k_data;
+    uint32_t* root_of = (uint32_t*)xcalloc(kd + K + 1, 4);
+    uint32_t* order = (uint32_t*)xcalloc(kd + K + 1, 4);
+    uint32_t ne = 0;
+    for (uint32_t c = 0; c < kd; ++c) { root_of[ne] = (uint32_t)s->clabels[c]; order[ne] = ne; ++ne; }
+    for (uint32_t c = 0; c < K; ++c)
+        if (croot[c] != 0xFFFFFFFFu) { root_of[ne] = croot[c]; order[ne] = ne; ++ne; }
+    g_root_of = root_of;
+    qsort(order, ne, 4, cmp_root_entry);
+    int32_t* data_nl = (int32_t*)xcalloc(kd ? kd : 1, 4);
+    int32_t* carried_nl = (int32_t*)xcalloc(K ? K : 1, 4);
+    /* entry e < kd is data cluster e; entry kd + q is the q-th carried cluster in label order */
+    uint32_t* carried_label = (uint32_t*)xcalloc(K ? K : 1, 4);
+    {
+        uint32_t q = 0;
+        for (uint32_t c = 0; c < K; ++c)
+            if (croot[c] != 0xFFFFFFFFu) carried_label[q++] = c;
+    }
+    int32_t survivors = 0;
+    for (uint32_t j = 0; j < ne; ++j) {
+        const uint32_t e = order[j];
+        if (e < kd) {
+            const orc_cluster_data cd = s->cdata[e];
+            const float pot = cd.max - cd.min;
+            const int keep = pot >= s->rw_threshold && cd.count >= 2;
+            data_nl[e] = keep ? survivors++ : (int32_t)((uint32_t)s->smallest - j - 1u);
+        } else {
+            carried_nl[carried_label[e - kd]] = survivors++;
+        }
+    }
+    float mx = 0.0f;
+    for (uint32_t i = 0; i < s->n_act; ++i) {
+        const int32_t lab = s->act[i].label;
+        const uint32_t v = s->act[i].nix;
+        if (lab < 0 || (uint32_t)lab >= s->n) continue;
+        const int32_t c = s->lookup[lab];
+        const int32_t nl = data_nl[c];
+        s->act[i].label = nl;
+        s->labels[v] = nl;
+        if (nl < 0) continue;
+        if (s->mode == ORC_MODE_REF) {
+            const double avg = (double)s->cdata[c].sum / (double)s->cdata[c].count;
+            s->xd[s->cur][v] -= avg;
+        } else {
+            const float xv = (float)((double)s->xf[v] - s->csum_fixed_avg[c]);
+            s->xf[v] = xv;
+            const float a = fabsf(xv);
+            if (a > mx) mx = a;
+        }
+    }
+    for (uint32_t j = 0; j < nc; ++j) {
+        const uint32_t v = carried[j].nix;
+        const int32_t nl = carried_nl[carried[j].label];
+        carried[j].label = nl;
+        s->labels[v] = nl;
+        if (s->mode == ORC_MODE_PXR) {
+            const float a = fabsf(s->xf[v]);
+            if (a > mx) mx = a;
+        }
+    }
+    if (s->mode == ORC_MODE_PXR) s->xmax = mx;
+    orc_disable_stage(s);   /* rows of the swept, kept vertices */
+    memcpy(s->act + s->n_act, carried, (size_t)nc * sizeof(orc_lnode));
+    s->n_act += nc;
+    s->n_clusters = (uint32_t)survivors;
+    free(carried); free(croot); free(root_of); free(order); free(data_nl); free(carried_nl); free(carried_label);
+}
+
 uint32_t orc_decompose(orc_state* s, uint32_t max_rounds) {
     uint32_t rounds = 0;
     while (rounds < max_rounds && s->n_clusters > 0 && s->n_act > 0) {

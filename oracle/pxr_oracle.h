@@ -70,6 +70,12 @@ void orc_cut_clusters(orc_state* s);   /* the five stages above */
 /* Re-emit the walk's sort keys from the current potentials. */
 void orc_rekey(orc_state* s);
 
+/* One round with a sweep schedule: due[c] != 0 for the active clusters
+ * (labels 0..n_clusters-1) that are swept this round; the others only walk
+ * and are relabelled.  No reference counterpart (the learned stop
+ * predictor's schedule); with every cluster due it is the plain round. */
+void orc_scheduled_round(orc_state* s, const uint8_t* due);
+
 /* Rounds until no active cluster is left (cuda/device.h:363-404). Returns the
  * number of rounds that ran a walk step. */
 uint32_t orc_decompose(orc_state* s, uint32_t max_rounds);

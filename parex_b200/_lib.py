@@ -8,6 +8,8 @@ from __future__ import annotations
 import ctypes as C
 import os
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libparex_b200.so")
 
@@ -28,6 +30,8 @@ SYMBOLS = [
     "pxr_download_graph64", "pxr_download_degrees", "pxr_download_labels", "pxr_active_edge_map",
     "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
     "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
+    "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
+    "pxr_mlp_adam_step",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -52,7 +56,42 @@ class Stats(C.Structure):
                 ("clusters_with_cut", C.c_uint32), ("device_bytes", C.c_uint64),
                 ("last_decompose_ms", C.c_double), ("kernel_launches", C.c_uint64),
                 ("walk_vertices", C.c_uint64), ("walk_slots", C.c_uint64), ("walk_gathers", C.c_uint64),
-                ("sort_items", C.c_uint64), ("sort_passes", C.c_uint64)]
+                ("sort_items", C.c_uint64), ("sort_passes", C.c_uint64), ("swept_items", C.c_uint64),
+                ("skipped_sweeps", C.c_uint64), ("false_stops", C.c_uint64)]
+
+
+MLP_FEATURES = 16
+MLP_HIDDEN = 32
+MLP_PARAMS = 1633
+SCHEDULE_PLAIN, SCHEDULE_LEARNED, SCHEDULE_AUDIT = 0, 1, 2
+
+
+class Schedule(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("trace", C.c_uint32), ("safety", C.c_float), ("max_skip", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
+
+
+class ClusterRecord(C.Structure):
+    _fields_ = [("root", C.c_uint32), ("size", C.c_uint32), ("volume", C.c_uint32), ("origin", C.c_uint32),
+                ("potential", C.c_float), ("sparsity", C.c_float), ("prev_potential", C.c_float),
+                ("prev_sparsity", C.c_float), ("prev_round", C.c_uint32), ("age", C.c_uint32),
+                ("round", C.c_uint32), ("skip", C.c_uint32), ("prediction", C.c_float), ("has_prev", C.c_uint32),
+                ("reserved", C.c_uint32 * 2), ("features", C.c_float * MLP_FEATURES)]
+
+
+class MlpLoss(C.Structure):
+    _fields_ = [("delta", C.c_float), ("over_weight", C.c_float)]
+
+
+class MlpAdam(C.Structure):
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
+
+
+RECORD_DTYPE = np.dtype([("root", "<u4"), ("size", "<u4"), ("volume", "<u4"), ("origin", "<u4"),
+                         ("potential", "<f4"), ("sparsity", "<f4"), ("prev_potential", "<f4"),
+                         ("prev_sparsity", "<f4"), ("prev_round", "<u4"), ("age", "<u4"), ("round", "<u4"),
+                         ("skip", "<u4"), ("prediction", "<f4"), ("has_prev", "<u4"), ("reserved", "<u4", 2),
+                         ("features", "<f4", MLP_FEATURES)])
 
 
 class PhaseStat(C.Structure):
@@ -112,10 +151,18 @@ def load() -> C.CDLL:
     L.pxr_set_potentials.argtypes = [p, p]
     L.pxr_set_state.argtypes = [p, p, p, u32, p, p, p, u32, i32, C.c_int]
     L.pxr_initialize_batched.argtypes = [p, u32, u64, p, p, u32, p]
+    L.pxr_set_schedule.argtypes = [p, C.POINTER(Schedule), p, p]
+    L.pxr_read_cluster_records.argtypes = [p, p, u32, C.POINTER(u32)]
+    L.pxr_mlp_forward.argtypes = [p, u32, p, p, p, p]
+    L.pxr_mlp_scratch_floats.argtypes = [u32]
+    L.pxr_mlp_gradient.argtypes = [p, p, u32, p, p, C.POINTER(MlpLoss), p, p, p, p]
+    L.pxr_mlp_adam_step.argtypes = [p, p, p, p, p, u32, C.POINTER(MlpAdam), p]
     for name in SYMBOLS:
         fn = getattr(L, name)
-        if name not in ("pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_destroy"):
+        if name not in ("pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_destroy",
+                        "pxr_mlp_scratch_floats"):
             fn.restype = C.c_int
+    L.pxr_mlp_scratch_floats.restype = C.c_size_t
     _lib = L
     return L
 

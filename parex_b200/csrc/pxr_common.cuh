@@ -21,6 +21,9 @@ enum : uint32_t {
 // Spin bound for every device-side wait (about a second with the back-off below).
 constexpr uint32_t kSpinLimit = 1u << 20;
 
+// Look-back sites (dynamic tile counters and epochs), one per scan kernel.
+constexpr int kSites = 12;
+
 // Per-round scalars kept on the device so rounds need no host round trip.
 struct RoundCtr {
     uint32_t n_active;        // active vertices (sweep input size)
@@ -35,7 +38,7 @@ struct RoundCtr {
     uint32_t xmax_walk_bits;  // max |x'| written by the last walk (float bits)
     uint32_t full_components; // run components over every cluster in the next cut
     uint32_t err;             // kErr* bits
-    uint32_t tile_counter[8]; // dynamic tile ids for look-back kernels
+    uint32_t tile_counter[kSites]; // dynamic tile ids for look-back kernels
     uint32_t rounds;          // rounds completed
     uint32_t done;            // set when no active cluster is left
     uint32_t main_sel;        // buffer holding the last sweep's sorted keys and values
@@ -43,12 +46,17 @@ struct RoundCtr {
     uint32_t sweep_k;         // clusters of the last sweep
     uint32_t loop_start;      // rounds at the start of the device-driven loop
     uint32_t loop_cap;        // round cap of the device-driven loop
+    uint32_t n_sweep;         // vertices in this round's sweep (all active ones in the plain form)
+    uint32_t n_due_items;     // vertices of the clusters swept and acted on this round
     uint32_t pad0;
     unsigned long long stat_walk_vertices;  // traffic counters since initialisation
     unsigned long long stat_walk_slots;
     unsigned long long stat_walk_gathers;
     unsigned long long stat_sort_items;
     unsigned long long stat_sort_passes;
+    unsigned long long stat_swept_items;     // sweep input vertices, summed over rounds
+    unsigned long long stat_skipped;         // cluster-rounds whose sweep the schedule skipped
+    unsigned long long stat_false_stops;     // skipped sweeps that would have cut (audit mode)
 };
 
 // ---------------------------------------------------------------------------

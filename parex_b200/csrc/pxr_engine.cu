@@ -8,12 +8,11 @@
 #include <string>
 #include <vector>
 
-#include "pxr_kernels.cuh"
+#include "pxr_sched.cuh"
 
 using namespace pxr;
 
 namespace pxr {
-constexpr int kSiteFinal = 5;
 constexpr uint32_t kMaxGrid = 148u * 32u;
 
 // ---------------------------------------------------------------------------
@@ -235,7 +234,7 @@ struct pxr_handle {
     uint8_t* split = nullptr;
     pxr_sweep_cut* allcuts = nullptr;
     uint32_t* roots[2] = {nullptr, nullptr};
-    LookbackState lb[6]{};
+    LookbackState lb[kSiteCarry + 1]{};
     uint32_t* lb_epoch = nullptr;
     RoundCtr* ctr = nullptr;
     SortState sort{};
@@ -250,6 +249,15 @@ struct pxr_handle {
     uint32_t* d_check = nullptr;   // [3]: invalid-input bits, max row length, heavy rows
     uint32_t* heavy = nullptr;     // vertices with more than kHeavyRow slots
     uint32_t n_heavy = 0;
+    // learned sweep schedule
+    pxr_schedule sched{};
+    uint8_t* sflag = nullptr;
+    uint8_t* nflag = nullptr;
+    uint32_t* rootc = nullptr;
+    float* mlp = nullptr;             // kMlpImage floats
+    std::vector<float> mlp_img;       // host copy (set before or after allocation)
+    pxr_cluster_record* records = nullptr;   // n entries, allocated when trace is first enabled
+    uint32_t records_n = 0;
     int xcur = 0, tcur = 0, acur = 0;
     int sweep_tab = 0;
     cudaGraphExec_t graphs[8] = {};  // device-driven loop, one per parity combination
@@ -305,6 +313,8 @@ void release(pxr_handle* h) {
     drop_graphs(h);
     for (void* p : h->allocs) cudaFree(p);
     h->allocs.clear();
+    h->records = nullptr;
+    h->records_n = 0;
     h->bytes = 0;
     h->initialized = false;
 }
@@ -349,6 +359,18 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.root_end_bit = h->root_end_bit;
     d.heavy = h->heavy;
     d.n_heavy = h->n_heavy;
+    d.sched = h->sched.mode;
+    d.trace = (h->sched.trace && h->records) ? 1u : 0u;
+    d.sflag = h->sflag;
+    d.nflag = h->nflag;
+    d.rootc = h->rootc;
+    d.lb_sched = h->lb[kSiteSched];
+    d.lb_emit = h->lb[kSiteEmit];
+    d.lb_carry = h->lb[kSiteCarry];
+    d.mlp = h->mlp;
+    d.safety = h->sched.safety;
+    d.max_skip = h->sched.max_skip;
+    d.records = h->records;
     return d;
 }
 
@@ -357,11 +379,11 @@ Dev<OffT> make_dev(pxr_handle* h) {
 
 enum Phase {
     kPhWalk, kPhNodeDiff, kPhEmit, kPhSort, kPhScan, kPhClusterCut, kPhCutInit, kPhUnion,
-    kPhComponents, kPhRootSort, kPhRelabel, kPhApply, kPhDisable, kPhCvol, kPhBook, kPhaseCount
+    kPhComponents, kPhRootSort, kPhRelabel, kPhApply, kPhDisable, kPhCvol, kPhBook, kPhSched, kPhaseCount
 };
 const char* kPhaseNames[kPhaseCount] = {"walk", "nodediff", "emit_keys", "sort", "sweep_scan", "cluster_cut",
                                         "cut_init", "union", "components", "root_sort", "relabel", "apply",
-                                        "disable", "cvol_scan", "bookkeeping"};
+                                        "disable", "cvol_scan", "bookkeeping", "schedule"};
 
 cudaEvent_t take_event(pxr_handle* h) {
     if (!h->event_pool.empty()) {
@@ -408,7 +430,7 @@ cudaError_t op_walk(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1); });
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
     const uint32_t hgrid = std::min(h->n_heavy, 148u * 16u);
     phase(h, kPhWalk, h->n_heavy ? 2 : 1, [&] {
         k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
@@ -426,24 +448,29 @@ cudaError_t op_sweep(pxr_handle* h) {
     cudaStream_t s = h->stream;
     const ClusterTables& t = h->tab[h->tcur];
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1); });
+    const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
+    if (h->sched.mode)
+        phase(h, kPhSched, 1, [&] { k_due_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t); });
     phase(h, kPhNodeDiff, h->n_heavy ? 2 : 1, [&] {
         k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
         if (h->n_heavy) k_nodediff_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d);
     });
     phase(h, kPhEmit, 1, [&] {
-        k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+        if (h->sched.mode)
+            k_emit_sched<OffT><<<tiles, kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+        else
+            k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
     });
     SortBuffers<uint64_t> b{};
     b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
     b.vals[0] = h->vals[0]; b.vals[1] = h->vals[1];
-    b.count = &h->ctr->n_active;
+    b.count = &h->ctr->n_sweep;
     b.end_bit = h->sort_end_bit;
     b.capacity = h->n;
     cudaError_t e = cudaSuccess;
     phase(h, kPhSort, 2 + kMaxPasses, [&] { e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64); });
     if (e != cudaSuccess) return e;
-    const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     phase(h, kPhScan, 1, [&] {
         k_sweep_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->keys[0], h->keys[1], h->vals[0], h->vals[1]);
     });
@@ -460,7 +487,9 @@ cudaError_t op_cut(pxr_handle* h) {
     const ClusterTables& nt = h->tab[h->tcur ^ 1];
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 2); });
+    if (h->sched.mode)
+        phase(h, kPhSched, 1, [&] { k_carry_roots<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->roots[0]); });
     phase(h, kPhCutInit, 1, [&] {
         k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });
@@ -488,7 +517,11 @@ cudaError_t op_cut(pxr_handle* h) {
         e = radix_sort<uint32_t>(rb, rs, &h->ctr->err, s, root_bits);
     });
     if (e != cudaSuccess) return e;
-    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], h->roots[1], nt); });
+    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], h->roots[1], t, nt); });
+    if (h->sched.mode)
+        phase(h, kPhSched, 1, [&] {
+            k_carry_vertices<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->act[h->acur], h->act[h->acur ^ 1]);
+        });
     phase(h, kPhApply, 1, [&] {
         k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
                                                h->act[h->acur ^ 1]);
@@ -499,6 +532,8 @@ cudaError_t op_cut(pxr_handle* h) {
             k_disable_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d, h->xt[h->xcur], nt);
     });
     phase(h, kPhCvol, 1, [&] { k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt); });
+    if (h->sched.mode || d.trace)
+        phase(h, kPhSched, 1, [&] { k_schedule<OffT><<<std::min(grid_for(h->n), 148u * 8u), kBlock, 0, s>>>(d, t, nt); });
     phase(h, kPhBook, 1, [&] { k_round_end<OffT><<<1, 1, 0, s>>>(d); });
     h->tcur ^= 1;
     h->acur ^= 1;
@@ -651,6 +686,16 @@ pxr_status decompose_stream(pxr_handle* h) {
 
 // ---------------------------------------------------------------------------
 
+// every cluster due, no sweep history (after any change of the partition state)
+pxr_status reset_schedule_state(pxr_handle* h) {
+    const size_t N = std::max<uint32_t>(h->n, 1);
+    for (int i = 0; i < 2; ++i) {
+        PXR_CUDA(h, cudaMemsetAsync(h->tab[i].skip, 0, N * sizeof(uint16_t), h->stream));
+        PXR_CUDA(h, cudaMemsetAsync(h->tab[i].hist, 0, N * sizeof(SchedHist), h->stream));
+    }
+    return PXR_OK;
+}
+
 pxr_status setup_tables_initial(pxr_handle* h) {
     // one cluster with every vertex: start 0, size n, volume 2m, root 0
     std::vector<uint32_t> one = {0u, h->n, (uint32_t)h->slots, 0u, 0u};
@@ -684,11 +729,15 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     for (int i = 0; i < 2; ++i) {
         A(&h->act[i], N); A(&h->ids[i], N); A(&h->keys[i], N); A(&h->vals[i], N); A(&h->roots[i], N);
         A(&h->tab[i].start, N); A(&h->tab[i].size, N); A(&h->tab[i].vol, N); A(&h->tab[i].vol_start, N);
-        A(&h->tab[i].root, N); A(&h->tab[i].best, N);
+        A(&h->tab[i].root, N); A(&h->tab[i].best, N); A(&h->tab[i].skip, N); A(&h->tab[i].hist, N);
     }
+    A(&h->sflag, N); A(&h->nflag, N); A(&h->rootc, N); A(&h->mlp, (size_t)kMlpImage);
+    if (h->sched.trace) { A(&h->records, N); }
     A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N);
-    for (int i = 0; i < 6; ++i) { A(&h->lb[i].flags, scan_tiles); A(&h->lb[i].agg, scan_tiles); A(&h->lb[i].inc, scan_tiles); }
-    A(&h->lb_epoch, 8); A(&h->ctr, 1);
+    for (int i = 0; i <= kSiteCarry; ++i) {
+        A(&h->lb[i].flags, scan_tiles); A(&h->lb[i].agg, scan_tiles); A(&h->lb[i].inc, scan_tiles);
+    }
+    A(&h->lb_epoch, kSites); A(&h->ctr, 1);
     A(&h->sort.hist, kMaxPasses * kRadix); A(&h->sort.bases, kMaxPasses * kRadix);
     A(&h->sort.pass_info, kMaxPasses + 1); A(&h->sort.tile_ctr, kMaxPasses); A(&h->sort.epoch, 1);
     A(&h->sort.status, (size_t)sort_tiles * kRadix);
@@ -701,8 +750,11 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     // look-back flags and sort status words carry epochs that only grow, so
     // they are cleared once here and never again
     cudaStream_t s = h->stream;
-    for (int i = 0; i < 6; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
-    PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, 8 * 4, s));
+    for (int i = 0; i <= kSiteCarry; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, kSites * 4, s));
+    h->records_n = h->records ? (uint32_t)N : 0u;
+    if (!h->mlp_img.empty())
+        PXR_CUDA(h, cudaMemcpyAsync(h->mlp, h->mlp_img.data(), kMlpImage * 4, cudaMemcpyHostToDevice, s));
     PXR_CUDA(h, cudaMemsetAsync(h->ctr, 0, sizeof(RoundCtr), s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.hist, 0, kMaxPasses * kRadix * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.epoch, 0, 4, s));
@@ -780,6 +832,7 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
         h->launches += 3;
     }
     pxr_status st = setup_tables_initial(h);
+    if (st == PXR_OK) st = reset_schedule_state(h);
     if (st != PXR_OK) return st;
     PXR_CUDA(h, cudaGetLastError());
     if (batched) return PXR_OK;   // batch_setup completes the state
@@ -1173,6 +1226,9 @@ pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out) {
     out->walk_gathers = h->h_ctr->stat_walk_gathers;
     out->sort_items = h->h_ctr->stat_sort_items;
     out->sort_passes = h->h_ctr->stat_sort_passes;
+    out->swept_items = h->h_ctr->stat_swept_items;
+    out->skipped_sweeps = h->h_ctr->stat_skipped;
+    out->false_stops = h->h_ctr->stat_false_stops;
     return st;
 }
 
@@ -1266,7 +1322,60 @@ pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* a
     c->full_components = full_components ? 1u : 0u;
     c->done = (n_act == 0 || n_clusters == 0) ? 1u : 0u;
     PXR_CUDA(h, cudaMemcpyAsync(h->ctr, c, sizeof(RoundCtr), cudaMemcpyHostToDevice, s));
+    pxr_status rs = reset_schedule_state(h);
+    if (rs != PXR_OK) return rs;
     return pxr_set_potentials(h, x);
+}
+
+pxr_status pxr_set_schedule(pxr_handle* h, const pxr_schedule* cfg, const uint16_t* weights, const float* norm) {
+    if (!h || !cfg) return PXR_INVALID_ARG;
+    if (cfg->mode > PXR_SCHEDULE_AUDIT) return fail(h, PXR_INVALID_ARG, "unknown schedule mode");
+    if (cfg->mode != PXR_SCHEDULE_PLAIN) {
+        if (!weights || !norm) return fail(h, PXR_INVALID_ARG, "the learned schedule needs weights and norm");
+        if (!(cfg->safety >= 0.0f) || cfg->max_skip > 0xFFFFu)
+            return fail(h, PXR_INVALID_ARG, "safety must be >= 0 and max_skip below 65536");
+        std::vector<float> img(kMlpImage);
+        for (int p = 0; p < kMlpParams; ++p) {
+            const uint32_t b = (uint32_t)weights[p] << 16;
+            std::memcpy(&img[p], &b, 4);
+        }
+        for (int i = 0; i < 2 * kMlpIn; ++i) img[kMlpParams + i] = norm[i];
+        h->mlp_img = std::move(img);
+    }
+    const bool mode_changed = cfg->mode != h->sched.mode || (cfg->trace != 0) != (h->sched.trace != 0);
+    h->sched = *cfg;
+    if (mode_changed) drop_graphs(h);   // the captured round depends on the mode
+    if (!h->allocs.empty()) {
+        PXR_CUDA(h, cudaSetDevice(h->device));
+        if (!h->mlp_img.empty())
+            PXR_CUDA(h, cudaMemcpyAsync(h->mlp, h->mlp_img.data(), kMlpImage * 4, cudaMemcpyHostToDevice, h->stream));
+        if (cfg->trace && !h->records) {
+            const size_t N = std::max<uint32_t>(h->n, 1);
+            cudaError_t e = dalloc(h, &h->records, N);
+            if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+            h->records_n = (uint32_t)N;
+            drop_graphs(h);
+        }
+        PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    return PXR_OK;
+}
+
+pxr_status pxr_read_cluster_records(pxr_handle* h, pxr_cluster_record* out, uint32_t cap, uint32_t* count) {
+    if (!h || !count || (cap && !out)) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    if (!h->sched.trace || !h->records) return fail(h, PXR_INVALID_ARG, "trace is off");
+    pxr_status st = sync_ctr(h);
+    if (st != PXR_OK) return st;
+    const uint32_t k = h->h_ctr->n_clusters;
+    *count = k;
+    const uint32_t w = std::min(cap, k);
+    if (w) {
+        PXR_CUDA(h, cudaMemcpyAsync(out, h->records, (size_t)w * sizeof(pxr_cluster_record), cudaMemcpyDeviceToHost,
+                                    h->stream));
+        PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    return PXR_OK;
 }
 
 }  // extern "C"

@@ -135,19 +135,25 @@ __device__ __forceinline__ uint32_t sorted_sel(const SortState& s) { return s.pa
 // ---------------------------------------------------------------------------
 // round bookkeeping
 
+// stage: 0 before the walk, 1 before the sweep, 2 before the cut
 template <typename OffT>
-__global__ void k_round_prep(Dev<OffT> d, int walk) {
+__global__ void k_round_prep(Dev<OffT> d, int stage) {
     RoundCtr* c = d.ctr;
     c->n_cut = 0;
     c->n_roots = 0;
-    if (walk) c->xmax_walk_bits = 0;
+    if (stage == 0) c->xmax_walk_bits = 0;
     c->smallest_next = 0;
     c->n_keep = 0;
     c->n_active_next = 0;
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < kSites; ++i) {
         c->tile_counter[i] = 0;
         d.lb_epoch[i] += 1;
     }
+    if (stage == 1) {
+        c->n_due_items = 0;
+        if (d.sched) c->n_sweep = 0;   // set by k_due_scan
+    }
+    if (!d.sched) c->n_sweep = c->n_active;
     const uint32_t k = c->n_clusters;
     *d.sort_end_bit = 32u + bitlen(k > 0 ? k - 1 : 0);
 }
@@ -158,7 +164,10 @@ __global__ void k_after_walk(Dev<OffT> d) { d.ctr->xmax_bits = d.ctr->xmax_walk_
 template <typename OffT>
 __global__ void k_round_end(Dev<OffT> d) {
     RoundCtr* c = d.ctr;
-    if (c->n_active > 0) c->rounds += 1;
+    if (c->n_active > 0) {
+        c->rounds += 1;
+        c->stat_swept_items += c->n_sweep;
+    }
     c->n_active = c->n_active_next;
     c->n_clusters = c->n_keep;
     c->smallest = c->smallest_next;
@@ -252,10 +261,12 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
     for (uint32_t j0 = warp0; j0 < count; j0 += groups) {
         const uint32_t j = j0 + (threadIdx.x & 31u) / W;
         const bool valid = j < count;
-        const uint32_t v = valid ? ids[j] : 0u;
-        const uint32_t mine = valid ? ordered_bits(d.x[v]) : 0u;
-        OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
-        const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
+        uint32_t v = valid ? ids[j] : 0u;
+        const bool in = valid && (!d.sched || ((uint32_t)d.lab[v] < d.n && (d.sflag[d.lab[v]] & 2u)));
+        if (!in) v = 0u;
+        const uint32_t mine = in ? ordered_bits(d.x[v]) : 0u;
+        OffT beg = in ? d.off[v] : 0, end = in ? d.off[v + 1] : 0;
+        const bool light = in && (uint64_t)(end - beg) <= kHeavyRow;
         if (!light) beg = end;      // heavy rows: k_nodediff_heavy
         int32_t c = 0;
         for (OffT s = beg + gl; s < end; s += 4 * W) {
@@ -306,7 +317,7 @@ __global__ void __launch_bounds__(kBlock) k_sweep_scan(Dev<OffT> d, ClusterTable
                                                        const uint32_t* vals1) {
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
     const uint32_t tile = fetch_tile(d.ctr, kSiteScan);
     if (tile >= ntiles) return;
@@ -390,20 +401,24 @@ __global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTabl
     const uint32_t full = d.ctr->full_components;
     pxr_sweep_cut* cuts = reinterpret_cast<pxr_sweep_cut*>(d.allcuts);
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < k; c += gridDim.x * blockDim.x) {
+        const uint32_t fl = d.sched ? d.sflag[c] : 3u;   // bit 0 acted on, bit 1 swept
+        const bool acted = fl & 1u, swept = fl & 2u;
         const uint64_t b = t.best[c];
         const uint32_t pos = ~(uint32_t)b;
-        const float sp = __uint_as_float((uint32_t)(b >> 32));
-        const uint32_t off = pos - t.start[c] + 1u;
+        const float sp = swept ? __uint_as_float((uint32_t)(b >> 32)) : 2.0f;
+        const uint32_t off = swept ? pos - t.start[c] + 1u : 0u;
         cuts[c].label = (int32_t)c;
         cuts[c].sparsity = sp;
         cuts[c].offset = off;
-        const bool cut = sp < d.sc_threshold;
+        const bool cut = acted && sp < d.sc_threshold;
         d.cut_off[c] = cut ? off : kNoCut;
-        const bool split = cut || full;
+        const bool split = acted && (cut || full);
         d.split[c] = split ? 1 : 0;
         const uint32_t cuts_in_warp = __ballot_sync(__activemask(), cut);
         if (cut && (cuts_in_warp & lanemask_lt()) == 0u) atomicAdd(&d.ctr->n_cut, (uint32_t)__popc(cuts_in_warp));
-        if (!split) {
+        if (!acted && swept && sp < d.sc_threshold) atomicAdd(&d.ctr->stat_false_stops, 1ull);
+        if (acted && !split && (d.sched || d.trace)) d.rootc[t.root[c]] = (kOriginSwept << 30) | c;
+        if (acted && !split) {
             const uint32_t r = t.root[c];
             d.acc_max[r] = 0u;
             d.acc_min[r] = 0xFFFFFFFFu;
@@ -422,7 +437,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cut_init(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                      const uint32_t* vals1, const uint64_t* keys0,
                                                      const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
@@ -463,7 +478,7 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t v) {
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
                                                        const uint64_t* keys0, const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
     const uint64_t* keys = sel ? keys1 : keys0;
@@ -486,7 +501,7 @@ __global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
                                                      const uint64_t* keys0, const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
     const uint64_t* keys = sel ? keys1 : keys0;
@@ -504,7 +519,7 @@ __global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
                                                   const uint64_t* keys0, const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
     const uint64_t* keys = sel ? keys1 : keys0;
@@ -539,7 +554,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                             const uint32_t* vals1, const uint64_t* keys0,
                                                             const uint64_t* keys1, uint32_t* roots) {
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
     const uint64_t* keys = sel ? keys1 : keys0;
@@ -558,12 +573,16 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
             const uint32_t i = first + k;
             if (i >= count) break;
             const uint32_t c = (uint32_t)(keys[i] >> 32);
+            if (d.sched && !(d.sflag[c] & 1u)) continue;   // carried (swept for the audit only)
             const uint32_t v = vals[i];
             uint32_t r;
             if (d.split[c]) {
                 r = uf_find(d.parent, v);
                 atomicMin(&d.parent[v], r);
-                if (r == v) my_roots[n_my++] = r;
+                if (r == v) {
+                    my_roots[n_my++] = r;
+                    if (d.sched || d.trace) d.rootc[r] = (kOriginChild << 30) | c;
+                }
             } else {
                 r = t.root[c];
                 if (i == t.start[c]) my_roots[n_my++] = r;
@@ -606,7 +625,7 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t* roots0, const uint32_t* roots1,
-                                                    ClusterTables nt) {
+                                                    ClusterTables t, ClusterTables nt) {
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_roots;
@@ -667,6 +686,18 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
             nt.root[nl] = r;
             nt.best[nl] = ~0ull;
             nt.vol[nl] = 0u;
+            if (d.sched) {
+                const uint32_t info = d.rootc[r];
+                const bool carried = (info >> 30) == kOriginCarried;
+                d.nflag[nl] = carried ? 1u : 0u;
+                if (carried) {
+                    const uint32_t c = info & kOriginLabelMask;
+                    nt.vol[nl] = t.vol[c];
+                    const uint16_t sk = t.skip[c];
+                    nt.skip[nl] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+                    nt.hist[nl] = t.hist[c];
+                }
+            }
         } else {
             const int32_t nl = (int32_t)((uint32_t)smallest - j - 1u);
             d.newlab[r] = nl;
@@ -687,7 +718,7 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
                                                   const uint64_t* keys1, uint32_t* act_next) {
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = d.ctr->n_sweep;
     const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
     const uint32_t tile = fetch_tile(d.ctr, kSiteApply);
     if (tile == 0 && threadIdx.x == 0) d.ctr->xmax_bits = 0;
@@ -705,6 +736,7 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
         vv[k] = 0;
         if (i >= count) continue;
         const uint32_t c = (uint32_t)(keys[i] >> 32);
+        if (d.sched && !(d.sflag[c] & 1u)) continue;   // carried: k_carry_vertices
         const uint32_t v = vals[i];
         vv[k] = v;
         // k_components_data left parent[v] at the root (atomicMin stores only
@@ -791,9 +823,10 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         const bool valid = q < nkept;
         const uint32_t v = valid ? s_list[q] : 0u;
         const int32_t lv = valid ? d.lab[v] : 0;
+        const bool carried = valid && d.sched && d.nflag[lv];   // rows, degree and x/d unchanged
         OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
         const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
-        if (!light) beg = end;      // heavy rows: k_disable_heavy
+        if (!light || carried) beg = end;      // heavy rows: k_disable_heavy
         uint32_t deg = 0;
         for (OffT s = beg + gl; s < end; s += 4 * W) {
             uint32_t nb[4];
@@ -811,7 +844,11 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         }
 #pragma unroll
         for (int o = W / 2; o > 0; o >>= 1) deg += __shfl_xor_sync(0xFFFFFFFFu, deg, o, W);
-        if (light && gl == 0) {
+        if (valid && carried && gl == 0) {
+            const uint32_t b = __float_as_uint(fabsf(d.x[v]));
+            vmax = b > vmax ? b : vmax;
+        }
+        if (light && !carried && gl == 0) {
             d.ideg[v] = deg;
             const float xv = d.x[v];
             xt[v] = deg ? __double2float_rn(__ddiv_rn((double)xv, (double)deg)) : 0.0f;
@@ -896,6 +933,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_heavy(Dev<OffT> d) {
     for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
         const uint32_t v = d.heavy[h];
         if (d.lab[v] < 0) continue;
+        if (d.sched && !(d.sflag[d.lab[v]] & 2u)) continue;
         const uint32_t mine = ordered_bits(d.x[v]);
         const OffT beg = d.off[v], end = d.off[v + 1];
         int32_t c = 0;
@@ -949,6 +987,10 @@ __global__ void __launch_bounds__(kBlock) k_disable_heavy(Dev<OffT> d, float* xt
         const uint32_t v = d.heavy[h];
         const int32_t lv = d.lab[v];
         if (lv < 0) continue;
+        if (d.sched && d.nflag[lv]) {   // carried: only its |x| counts
+            if (threadIdx.x == 0) atomicMax(&d.ctr->xmax_bits, __float_as_uint(fabsf(d.x[v])));
+            continue;
+        }
         const OffT beg = d.off[v], end = d.off[v + 1];
         uint32_t deg = 0;
         for (OffT s = beg + threadIdx.x; s < end; s += kBlock) {

@@ -26,6 +26,15 @@
 
 namespace pxr {
 
+// Sweep history of a cluster, carried across relabelling (the learned
+// schedule's features).
+struct SchedHist {
+    float pot;            // potential spread (max - min) at the last sweep
+    float sp;             // best sweep sparsity at the last sweep (2 when none)
+    uint32_t round;       // round of the last sweep
+    uint32_t age;         // sweeps since the cluster was created
+};
+
 struct ClusterTables {
     uint32_t* start;      // first sorted position of the cluster
     uint32_t* size;       // vertices
@@ -33,7 +42,14 @@ struct ClusterTables {
     uint32_t* vol_start;  // exclusive prefix of vol over labels
     uint32_t* root;       // minimum vertex id
     uint64_t* best;       // packed (sparsity bits, ~position) argmin
+    uint16_t* skip;       // learned schedule: rounds left before the next sweep
+    SchedHist* hist;      // learned schedule: sweep history
 };
+
+// Origin of a cluster after the round, stored at its root vertex
+// (Dev::rootc): kind << 30 | label of the cluster it came from.
+enum : uint32_t { kOriginSwept = 1u, kOriginChild = 2u, kOriginCarried = 3u };
+constexpr uint32_t kOriginLabelMask = 0x3FFFFFFFu;
 
 template <typename OffT>
 struct Dev {
@@ -75,6 +91,17 @@ struct Dev {
     uint32_t* root_end_bit;   // root sort bits
     const uint32_t* heavy;    // vertices whose row exceeds kHeavyRow slots (one CTA each)
     uint32_t n_heavy;
+    // learned sweep schedule (all zero / null in the plain form)
+    uint32_t sched;           // PXR_SCHEDULE_*
+    uint32_t trace;           // write per-cluster records each round
+    uint8_t* sflag;           // per label this round: bit 0 acted on (due), bit 1 in the sweep
+    uint8_t* nflag;           // per label of the next round: 1 when carried unswept
+    uint32_t* rootc;          // per root vertex: kind << 30 | old label
+    LookbackState lb_sched, lb_emit, lb_carry;
+    const float* mlp;         // bf16 weights widened to float, then input mean and scale
+    float safety;             // skip = floor(safety * (2^y - 1))
+    uint32_t max_skip;
+    void* records;            // pxr_cluster_record[] when trace is on
 };
 
 // Rows longer than this are processed by a whole CTA in the *_heavy kernels
@@ -82,7 +109,10 @@ struct Dev {
 constexpr uint32_t kHeavyRow = 64;
 
 // look-back sites (index into Dev::lb_epoch and RoundCtr::tile_counter)
-enum : int { kSiteScan = 0, kSiteRelabel = 1, kSiteApply = 2, kSiteIds = 3, kSiteCvol = 4 };
+enum : int {
+    kSiteScan = 0, kSiteRelabel = 1, kSiteApply = 2, kSiteIds = 3, kSiteCvol = 4,
+    kSiteFinal = 5, kSiteSched = 6, kSiteEmit = 7, kSiteCarry = 8
+};
 
 __device__ __forceinline__ uint32_t bitlen(uint32_t v) { return v ? 32u - __clz(v) : 0u; }
 

@@ -1,0 +1,276 @@
+// Kernels of the learned sweep schedule (sm_100a).  No reference
+// counterpart: the reference sweeps every active cluster every round.
+//
+// A cluster whose skip counter is non-zero is "carried" through the round:
+// its vertices walk with the rest, but it is left out of the sort, the scan,
+// the cut, components and recentering.  The clusters that are due go through
+// the unchanged plain kernels, restricted to the sweep set by the tables this
+// file builds (start and start volume of the due clusters only), so every cut
+// is still chosen and scored by the exact sweep.  Carried clusters keep their
+// vertices and rows and take part in the dense relabelling (root order over
+// all clusters).  After the round a per-cluster kernel evaluates the MLP on
+// the cluster's features and sets how many rounds it is carried next.
+// In audit mode every cluster is swept, the schedule only decides which
+// sweeps are acted on, and a skipped sweep that finds a cut is counted as a
+// false stop; the partition is the same as without the audit.
+#pragma once
+
+#include "pxr_kernels.cuh"
+#include "pxr_mlp.cuh"
+
+namespace pxr {
+
+// per cluster: due / in-sweep flags and the start tables of the sweep set
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_due_scan(Dev<OffT> d, ClusterTables t) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = d.ctr->n_clusters;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteSched);
+    if (tile >= ntiles) return;
+    const uint32_t epoch = d.lb_epoch[kSiteSched];
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint64_t vals[kScanItems];
+    uint64_t run = 0;
+    uint32_t due_items = 0, skipped = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t c = first + k;
+        uint64_t v = 0;
+        if (c < count) {
+            const bool due = t.skip[c] == 0;
+            const bool swept = due || d.sched == 2u;
+            d.sflag[c] = (uint8_t)((due ? 1u : 0u) | (swept ? 2u : 0u));
+            if (swept) v = ((uint64_t)t.vol[c] << 32) | t.size[c];
+            if (due) due_items += t.size[c]; else ++skipped;
+        }
+        vals[k] = v;
+        run = PairAdd::combine(run, v);
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<PairAdd>(d.lb_sched, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
+        if (threadIdx.x == 0 && tile == ntiles - 1) d.ctr->n_sweep = (uint32_t)PairAdd::combine(ex, tile_total);
+    }
+    __syncthreads();
+    const uint32_t lo = (uint32_t)incl - (uint32_t)run;
+    const uint32_t hi = (uint32_t)(incl >> 32) - (uint32_t)(run >> 32);
+    uint64_t p = PairAdd::combine(s_excl, ((uint64_t)hi << 32) | lo);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t c = first + k;
+        if (c >= count) break;
+        if (vals[k]) {
+            t.start[c] = (uint32_t)p;
+            t.vol_start[c] = (uint32_t)(p >> 32);
+        }
+        p = PairAdd::combine(p, vals[k]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        due_items += __shfl_xor_sync(0xFFFFFFFFu, due_items, o);
+        skipped += __shfl_xor_sync(0xFFFFFFFFu, skipped, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (due_items) atomicAdd(&d.ctr->n_due_items, due_items);
+        if (skipped) atomicAdd(&d.ctr->stat_skipped, (unsigned long long)skipped);
+    }
+}
+
+// sort keys of the sweep set, compacted from the last sort order
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_emit_sched(Dev<OffT> d, const uint32_t* act, uint64_t* keys,
+                                                       uint32_t* vals, uint64_t* best) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t k = d.ctr->n_clusters;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < k; c += gridDim.x * blockDim.x) best[c] = ~0ull;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteEmit);
+    if (tile >= ntiles) return;
+    const uint32_t epoch = d.lb_epoch[kSiteEmit];
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint64_t kk[kScanItems];
+    uint32_t vv[kScanItems];
+    uint32_t mask = 0, run = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        const uint32_t i = first + q;
+        kk[q] = 0;
+        vv[q] = 0;
+        if (i >= count) continue;
+        const uint32_t v = act[i];
+        const uint32_t c = (uint32_t)d.lab[v];
+        if (c < k && (d.sflag[c] & 2u)) {
+            kk[q] = ((uint64_t)c << 32) | ordered_bits(d.x[v]);
+            vv[q] = v;
+            mask |= 1u << q;
+            ++run;
+        }
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &tile_total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(d.lb_emit, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
+    }
+    __syncthreads();
+    uint32_t pos = (uint32_t)(s_excl + incl - run);
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q)
+        if (mask & (1u << q)) {
+            keys[pos] = kk[q];
+            vals[pos] = vv[q];
+            ++pos;
+        }
+}
+
+// Carried clusters: register their roots for the relabelling with data that
+// keeps them (count = size, spread 2, sum 0).
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTables t, uint32_t* roots) {
+    const uint32_t k = d.ctr->n_clusters;
+    for (uint32_t c0 = blockIdx.x * blockDim.x; c0 < k; c0 += gridDim.x * blockDim.x) {
+        const uint32_t c = c0 + threadIdx.x;
+        const bool carried = c < k && !(d.sflag[c] & 1u);
+        uint32_t r = 0;
+        if (carried) {
+            r = t.root[c];
+            d.acc_cnt[r] = t.size[c];
+            d.acc_max[r] = ordered_bits(1.0f);
+            d.acc_min[r] = ordered_bits(-1.0f);
+            d.acc_sum[r] = 0;
+            d.rootc[r] = (kOriginCarried << 30) | c;
+        }
+        const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, carried);
+        uint32_t slot = 0;
+        if ((threadIdx.x & 31u) == 0 && ballot) slot = atomicAdd(&d.ctr->n_roots, (uint32_t)__popc(ballot));
+        slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+        if (carried) roots[slot + __popc(ballot & lanemask_lt())] = r;
+    }
+}
+
+// Carried vertices: new label, and their place in the next active list after
+// the swept ones (in the order of the last sort).
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_carry_vertices(Dev<OffT> d, ClusterTables t, const uint32_t* act,
+                                                           uint32_t* act_next) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteCarry);
+    if (tile >= ntiles) return;
+    const uint32_t epoch = d.lb_epoch[kSiteCarry];
+    const uint32_t base = d.ctr->n_active_next - (count - d.ctr->n_due_items);
+    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t vv[kScanItems];
+    uint32_t mask = 0, run = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        const uint32_t i = first + q;
+        vv[q] = 0;
+        if (i >= count) continue;
+        const uint32_t v = act[i];
+        const uint32_t c = (uint32_t)d.lab[v];   // due vertices may carry cut labels k + c here
+        if (c < k && !(d.sflag[c] & 1u)) {
+            d.lab[v] = d.newlab[t.root[c]];
+            vv[q] = v;
+            mask |= 1u << q;
+            ++run;
+        }
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)run, warp_tot, &tile_total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(d.lb_carry, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) s_excl = ex;
+    }
+    __syncthreads();
+    uint32_t pos = base + (uint32_t)(s_excl + incl - run);
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q)
+        if (mask & (1u << q)) {
+            if (pos < d.n) act_next[pos] = vv[q];
+            else atomicOr(&d.ctr->err, kErrLabelRange);   // sizes and active list disagree
+            ++pos;
+        }
+}
+
+// After the round, per cluster of the next round: features, the sweep
+// history and, in the learned modes, the MLP's skip count.  Carried clusters
+// were already handled by k_relabel (counter decremented, history kept).
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock, 1) k_schedule(Dev<OffT> d, ClusterTables t, ClusterTables nt) {
+    __shared__ float img[kMlpImage];
+    if (d.sched)
+        for (int p = threadIdx.x; p < kMlpImage; p += blockDim.x) img[p] = d.mlp[p];
+    __syncthreads();
+    const uint32_t k = d.ctr->n_keep;
+    const uint32_t round = d.ctr->rounds;
+    pxr_cluster_record* rec = static_cast<pxr_cluster_record*>(d.records);
+    for (uint32_t nl = blockIdx.x * blockDim.x + threadIdx.x; nl < k; nl += gridDim.x * blockDim.x) {
+        const uint32_t r = nt.root[nl];
+        const uint32_t info = d.rootc[r];
+        const uint32_t kind = info >> 30;
+        const uint32_t c = info & kOriginLabelMask;
+        if (kind == kOriginCarried) {
+            if (d.trace) {
+                rec[nl].root = r;
+                rec[nl].size = nt.size[nl];
+                rec[nl].volume = nt.vol[nl];
+                rec[nl].origin = kind;
+                rec[nl].skip = nt.skip[nl];
+                rec[nl].round = round;
+            }
+            continue;
+        }
+        const uint32_t size = nt.size[nl];
+        const uint32_t vol = nt.vol[nl];
+        const float pot = __fsub_rn(from_ordered_bits(d.acc_max[r]), from_ordered_bits(d.acc_min[r]));
+        const float sp = __uint_as_float((uint32_t)(t.best[c] >> 32));
+        SchedHist h{0.0f, 2.0f, 0u, 0u};
+        if (kind == kOriginSwept) h = t.hist[c];
+        const bool has_prev = kind == kOriginSwept && h.age > 0;
+        const uint32_t dr = has_prev ? round - h.round : 0u;
+        float f[kMlpIn];
+        cluster_features(f, size, vol, pot, sp, has_prev, h.pot, h.sp, dr, kind == kOriginSwept ? h.age : 0u, round,
+                         d.rw_threshold, d.sc_threshold);
+        float y = 0.0f;
+        uint32_t sk = 0;
+        if (d.sched && kind == kOriginSwept) {
+            float z[kMlpIn], a1[kMlpHidden], h1[kMlpHidden], a2[kMlpHidden], h2[kMlpHidden];
+            y = mlp_forward(img, f, z, a1, h1, a2, h2);
+            sk = skip_from_prediction(y, d.safety, d.max_skip);
+        }
+        if (d.sched) nt.skip[nl] = (uint16_t)sk;
+        const SchedHist nh{pot, sp, round, kind == kOriginSwept ? h.age + 1u : 0u};
+        nt.hist[nl] = nh;
+        if (d.trace) {
+            pxr_cluster_record& o = rec[nl];
+            o.root = r;
+            o.size = size;
+            o.volume = vol;
+            o.origin = kind;
+            o.potential = pot;
+            o.sparsity = sp;
+            o.prev_potential = h.pot;
+            o.prev_sparsity = h.sp;
+            o.prev_round = h.round;
+            o.age = kind == kOriginSwept ? h.age : 0u;
+            o.round = round;
+            o.skip = sk;
+            o.prediction = y;
+            o.has_prev = has_prev ? 1u : 0u;
+#pragma unroll
+            for (int i = 0; i < kMlpIn; ++i) o.features[i] = f[i];
+        }
+    }
+}
+
+}  // namespace pxr

@@ -1,0 +1,342 @@
+"""Learned stop predictor: traces, GPU training and the learned schedule.
+
+The reference sweeps every active cluster in every round.  Most of those
+sweeps change nothing: on a 3D grid about four in five swept vertices belong
+to clusters that are neither cut nor certified in that round.  The learned
+schedule lets a cluster skip the sweep for the rounds a small MLP predicts,
+while its vertices keep walking; cuts are still chosen and scored by the
+exact sweep and certificates still come from the plain potential check
+(pxr_set_schedule in include/parex_b200.h).
+
+Pipeline (all GPU work in this package's own kernels):
+
+1. ``collect_trace``: the plain method runs round by round with trace records
+   (pxr_read_cluster_records): per active cluster its root, size and the 16
+   features the schedule reads.
+2. ``trace_targets``: for each swept cluster, the number of following rounds
+   in which the plain method's sweep left it unchanged; the target is
+   log2(1 + that count), the rounds a schedule could have skipped safely.
+3. ``train``: Adam on the asymmetric Huber loss (over-prediction weighted,
+   it is what costs cut quality) with pxr_mlp_gradient / pxr_mlp_adam_step;
+   the batch gather and the data stay in device memory (torch tensors as
+   plumbing).
+4. ``Model.save``/``load``: bf16 weight bits, input normalisation, metadata.
+
+``python -m parex_b200.learn train --out model.npz`` trains on the default
+trace graphs (planted partitions, grids and R-MAT graphs at seeds disjoint
+from the evaluation ones) and evaluates plain against learned on held-out
+graphs.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import sys
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from . import graphs as G
+from .manager import CudaDeviceManager
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_MODEL = os.path.join(HERE, "data", "stop_predictor.npz")
+F = _lib.MLP_FEATURES
+P = _lib.MLP_PARAMS
+ORIGIN_SWEPT, ORIGIN_CHILD, ORIGIN_CARRIED = 1, 2, 3
+
+
+# ----------------------------------------------------------------------------
+# model
+
+
+@dataclass
+class Model:
+    weights: np.ndarray                 # uint16 bf16 bit patterns, P entries
+    norm: np.ndarray                    # float32, 16 means then 16 scales
+    meta: dict = field(default_factory=dict)
+
+    def save(self, path: str) -> None:
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        np.savez(path, weights=self.weights.astype(np.uint16), norm=self.norm.astype(np.float32),
+                 meta=np.frombuffer(json.dumps(self.meta).encode(), dtype=np.uint8))
+
+    @staticmethod
+    def load(path: str = DEFAULT_MODEL) -> "Model":
+        z = np.load(path)
+        meta = json.loads(bytes(z["meta"]).decode()) if "meta" in z else {}
+        return Model(z["weights"].astype(np.uint16), z["norm"].astype(np.float32), meta)
+
+
+def init_master(seed: int = 0) -> np.ndarray:
+    """He-normal float32 master weights, zero biases, in the kernel layout."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(P, dtype=np.float32)
+    w[0:512] = rng.normal(0, math.sqrt(2.0 / F), 512)
+    w[544:1568] = rng.normal(0, math.sqrt(2.0 / 32), 1024)
+    w[1600:1632] = rng.normal(0, math.sqrt(1.0 / 32), 32)
+    return w
+
+
+def to_bf16_bits(x: np.ndarray) -> np.ndarray:
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16
+    return b.astype(np.uint16)
+
+
+# ----------------------------------------------------------------------------
+# traces
+
+
+def collect_trace(graph, seed: int, sc: float = 0.3, rw: float = 1e-4, device: int = 0,
+                  max_rounds: int = 10000) -> np.ndarray:
+    """Plain decomposition round by round; every round's cluster records."""
+    dm = CudaDeviceManager(seed=seed, sc_threshold=sc, rw_threshold=rw, device=device, driver=_lib.DRIVER_STREAM)
+    dm.set_schedule(_lib.SCHEDULE_PLAIN, trace=True)
+    dm.initialize(graph)
+    out = []
+    for _ in range(max_rounds):
+        if dm.getNumClusters() == 0:
+            break
+        dm.iterateRandomWalk()
+        dm.computeSweepCuts()
+        dm.cutClusters()
+        out.append(dm.cluster_records())
+    return np.concatenate(out) if out else np.zeros(0, dtype=_lib.RECORD_DTYPE)
+
+
+def trace_targets(rec: np.ndarray) -> np.ndarray:
+    """Safe skips of every record: the number of following rounds in which the
+    same vertex set (same root and size) was swept without being cut or
+    certified (-1 for records that are not swept clusters)."""
+    key = (rec["root"].astype(np.uint64) << np.uint64(32)) | rec["size"].astype(np.uint64)
+    rounds = rec["round"]
+    swept = rec["origin"] == ORIGIN_SWEPT
+    out = np.full(rec.shape[0], -1, dtype=np.int64)
+    later_keys = np.zeros(0, dtype=np.uint64)
+    later_t = np.zeros(0, dtype=np.int64)
+    for r in np.unique(rounds)[::-1]:
+        idx = np.nonzero((rounds == r) & swept)[0]
+        k = key[idx]
+        t = np.zeros(idx.shape[0], dtype=np.int64)
+        if later_keys.size:
+            pos = np.searchsorted(later_keys, k)
+            pos = np.minimum(pos, later_keys.size - 1)
+            hit = later_keys[pos] == k
+            t[hit] = later_t[pos[hit]] + 1
+        out[idx] = t
+        order = np.argsort(k)
+        later_keys, later_t = k[order], t[order]
+    return out
+
+
+def dataset(traces) -> tuple[np.ndarray, np.ndarray]:
+    xs, ts = [], []
+    for rec in traces:
+        t = trace_targets(rec)
+        keep = t >= 0
+        xs.append(rec["features"][keep].astype(np.float32))
+        ts.append(np.log2(1.0 + np.minimum(t[keep], 255)).astype(np.float32))
+    return np.concatenate(xs), np.concatenate(ts)
+
+
+# ----------------------------------------------------------------------------
+# training on the GPU (pxr_mlp_gradient + pxr_mlp_adam_step)
+
+
+def _dptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+def train(X: np.ndarray, T: np.ndarray, epochs: int = 40, batch: int = 8192, lr: float = 3e-3, seed: int = 0,
+          delta: float = 1.0, over: float = 4.0, device: int = 0, log=None) -> Model:
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda", device)
+    mean = X.mean(0)
+    std = X.std(0)
+    scale = np.where(std > 1e-6, 1.0 / np.maximum(std, 1e-6), 0.0).astype(np.float32)
+    norm = np.concatenate([mean.astype(np.float32), scale]).astype(np.float32)
+    Xd = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).to(dev)
+    Td = torch.from_numpy(np.ascontiguousarray(T, dtype=np.float32)).to(dev)
+    normd = torch.from_numpy(norm).to(dev)
+    master = torch.from_numpy(init_master(seed)).to(dev)
+    m = torch.zeros(P, dtype=torch.float32, device=dev)
+    v = torch.zeros(P, dtype=torch.float32, device=dev)
+    w = torch.from_numpy(to_bf16_bits(master.cpu().numpy()).view(np.int16)).to(dev)
+    grad = torch.zeros(P, dtype=torch.float32, device=dev)
+    lossd = torch.zeros(1, dtype=torch.float32, device=dev)
+    scratch = torch.zeros(int(L.pxr_mlp_scratch_floats(batch)), dtype=torch.float32, device=dev)
+    loss_spec = _lib.MlpLoss(delta, over)
+    opt = _lib.MlpAdam(lr, 0.9, 0.999, 1e-8)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    n = X.shape[0]
+    step = 0
+    history = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, device=dev, generator=gen)
+        tot = 0.0
+        nb = 0
+        for b0 in range(0, n - batch + 1 if n >= batch else 1, batch):
+            idx = perm[b0:b0 + batch]
+            xb = Xd.index_select(0, idx).contiguous()
+            tb = Td.index_select(0, idx).contiguous()
+            nbatch = xb.shape[0]
+            st = L.pxr_mlp_gradient(_dptr(xb), _dptr(tb), nbatch, _dptr(w), _dptr(normd), C.byref(loss_spec),
+                                    _dptr(scratch), _dptr(grad), _dptr(lossd), stream)
+            if st != 0:
+                raise _lib.PxrError(st, "pxr_mlp_gradient")
+            step += 1
+            st = L.pxr_mlp_adam_step(_dptr(master), _dptr(m), _dptr(v), _dptr(grad), _dptr(w), step, C.byref(opt),
+                                     stream)
+            if st != 0:
+                raise _lib.PxrError(st, "pxr_mlp_adam_step")
+            tot += float(lossd.item()) if nb % 16 == 0 else 0.0
+            nb += 1
+        history.append(tot)
+        if log:
+            log(f"epoch {ep}: sampled loss {tot:.4f}")
+    torch.cuda.synchronize(dev)
+    model = Model(w.cpu().numpy().view(np.uint16).copy(), norm,
+                  {"samples": int(n), "epochs": epochs, "batch": batch, "lr": lr, "delta": delta,
+                   "over_weight": over, "seed": seed, "steps": step})
+    return model
+
+
+def predict(model: Model, X: np.ndarray, device: int = 0) -> np.ndarray:
+    """Batch inference with pxr_mlp_forward."""
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda", device)
+    Xd = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).to(dev)
+    wd = torch.from_numpy(model.weights.view(np.int16).copy()).to(dev)
+    nd = torch.from_numpy(model.norm).to(dev)
+    out = torch.zeros(X.shape[0], dtype=torch.float32, device=dev)
+    st = L.pxr_mlp_forward(_dptr(Xd), X.shape[0], _dptr(wd), _dptr(nd), _dptr(out),
+                           C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    if st != 0:
+        raise _lib.PxrError(st, "pxr_mlp_forward")
+    return out.cpu().numpy()
+
+
+# ----------------------------------------------------------------------------
+# evaluation: plain against learned on one graph
+
+
+def cut_edges(graph, ids: np.ndarray) -> int:
+    """Undirected edges whose endpoints lie in different output clusters."""
+    src = np.repeat(np.arange(graph.n, dtype=np.int64), np.diff(graph.offsets.astype(np.int64)))
+    dst = graph.cols.astype(np.int64)
+    return int(np.count_nonzero(ids[src] != ids[dst]) // 2)
+
+
+def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, max_skip: int, device: int = 0,
+             reps: int = 1, driver: int = _lib.DRIVER_GRAPH, sc: float = 0.3, rw: float = 1e-4) -> dict:
+    import torch
+    dm = CudaDeviceManager(seed=seed, sc_threshold=sc, rw_threshold=rw, device=device, driver=driver)
+    if mode != _lib.SCHEDULE_PLAIN:
+        dm.set_schedule(mode, model.weights, model.norm, safety=safety, max_skip=max_skip)
+    times = []
+    rounds = 0
+    for _ in range(reps):
+        dm.initialize(graph)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        rounds = dm.expanderDecomposition()
+        times.append(dm.stats()["last_decompose_ms"])
+    fp = dm.getFinalPartition()
+    st = dm.stats()
+    return {"ms": min(times), "rounds": rounds, "clusters": fp.numClusters,
+            "cut_edges": cut_edges(graph, fp.clusterIds), "device_cut_edges": dm.getNumCutEdges(),
+            "swept_items": st["swept_items"], "skipped_sweeps": st["skipped_sweeps"],
+            "false_stops": st["false_stops"], "ids": fp.clusterIds}
+
+
+def compare(graph, model: Model, seed: int = 6582, safety: float = 0.5, max_skip: int = 16, device: int = 0,
+            reps: int = 3, audit: bool = True) -> dict:
+    plain = run_mode(graph, _lib.SCHEDULE_PLAIN, None, seed, safety, max_skip, device, reps)
+    learned = run_mode(graph, _lib.SCHEDULE_LEARNED, model, seed, safety, max_skip, device, reps)
+    res = {"graph": graph.name, "n": graph.n, "m": graph.m, "safety": safety, "max_skip": max_skip,
+           "plain": {k: v for k, v in plain.items() if k != "ids"},
+           "learned": {k: v for k, v in learned.items() if k != "ids"}}
+    res["speedup"] = plain["ms"] / learned["ms"] if learned["ms"] > 0 else None
+    res["cut_ratio"] = learned["cut_edges"] / max(plain["cut_edges"], 1)
+    res["swept_ratio"] = learned["swept_items"] / max(plain["swept_items"], 1)
+    if audit:
+        aud = run_mode(graph, _lib.SCHEDULE_AUDIT, model, seed, safety, max_skip, device, 1)
+        res["audit_identical"] = bool(np.array_equal(aud["ids"], learned["ids"]))
+        res["false_stop_rate"] = aud["false_stops"] / max(aud["skipped_sweeps"], 1)
+        res["false_stops"] = aud["false_stops"]
+        res["skipped_sweeps"] = aud["skipped_sweeps"]
+    return res
+
+
+TRAIN_GRAPHS = [
+    ("sbm16k", lambda s: G.sbm_graph(16384, 16, 12.0, 0.5, s), [11, 12, 13]),
+    ("grid48", lambda s: G.grid3d(48), [21, 22]),
+    ("grid64", lambda s: G.grid3d(64), [23]),
+    ("rmat16", lambda s: G.rmat(16, 16, seed=s), [31, 32]),
+]
+EVAL_GRAPHS = [
+    ("sbm16k_6582", lambda: G.sbm_graph(16384, 16, 12.0, 0.5, 6582), 6582),
+    ("grid128", lambda: G.grid3d(128), 6582),
+    ("rmat18", lambda: G.rmat(18, 16, seed=1), 6582),
+]
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m parex_b200.learn")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--out", default=DEFAULT_MODEL)
+    t.add_argument("--epochs", type=int, default=40)
+    t.add_argument("--batch", type=int, default=8192)
+    t.add_argument("--lr", type=float, default=3e-3)
+    t.add_argument("--over", type=float, default=4.0)
+    t.add_argument("--eval", action="store_true")
+    t.add_argument("--report", default=None)
+    e = sub.add_parser("eval")
+    e.add_argument("--model", default=DEFAULT_MODEL)
+    e.add_argument("--safety", type=float, nargs="*", default=[0.5])
+    e.add_argument("--max-skip", type=int, default=16)
+    e.add_argument("--report", default=None)
+    args = ap.parse_args(argv)
+    log = lambda s: print(s, file=sys.stderr, flush=True)
+    report = {}
+    if args.cmd == "train":
+        traces = []
+        for name, make, seeds in TRAIN_GRAPHS:
+            for s in seeds:
+                t0 = time.perf_counter()
+                rec = collect_trace(make(s), seed=s)
+                traces.append(rec)
+                log(f"trace {name} seed {s}: {rec.shape[0]} records, {time.perf_counter() - t0:.1f} s")
+        X, T = dataset(traces)
+        log(f"dataset: {X.shape[0]} samples, mean target {T.mean():.3f}")
+        model = train(X, T, epochs=args.epochs, batch=args.batch, lr=args.lr, over=args.over, log=log)
+        model.meta["train_graphs"] = [[n, s] for n, _, ss in TRAIN_GRAPHS for s in ss]
+        model.save(args.out)
+        report["train"] = model.meta
+        if args.eval:
+            report["eval"] = [compare(make(), model, seed=seed) for _, make, seed in EVAL_GRAPHS]
+    else:
+        model = Model.load(args.model)
+        report["eval"] = [compare(make(), model, seed=seed, safety=sf, max_skip=args.max_skip)
+                          for _, make, seed in EVAL_GRAPHS for sf in args.safety]
+    text = json.dumps(report, indent=1, default=float)
+    print(text)
+    if args.report:
+        with open(args.report, "w") as f:
+            f.write(text)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

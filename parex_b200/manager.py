@@ -223,6 +223,29 @@ class CudaDeviceManager:
         self._call(self._L.pxr_get_stats, C.byref(st))
         return {f: getattr(st, f) for f, _ in _lib.Stats._fields_}
 
+    def set_schedule(self, mode: int, weights=None, norm=None, safety: float = 0.5, max_skip: int = 16,
+                     trace: bool = False) -> None:
+        """Learned sweep schedule (pxr_set_schedule).  weights: MLP_PARAMS bf16
+        bit patterns (uint16); norm: 16 means then 16 scales."""
+        cfg = _lib.Schedule(mode, 1 if trace else 0, safety, max_skip)
+        w = n = None
+        if weights is not None:
+            w = np.ascontiguousarray(weights, dtype=np.uint16)
+            assert w.shape[0] == _lib.MLP_PARAMS
+            n = np.ascontiguousarray(norm, dtype=np.float32)
+            assert n.shape[0] == 2 * _lib.MLP_FEATURES
+        self._call(self._L.pxr_set_schedule, C.byref(cfg), _ptr(w) if w is not None else None,
+                   _ptr(n) if n is not None else None)
+
+    def cluster_records(self) -> np.ndarray:
+        """pxr_cluster_record of every active cluster after the last round (trace mode)."""
+        cnt = C.c_uint32(0)
+        self._call(self._L.pxr_read_cluster_records, None, 0, C.byref(cnt))
+        out = np.zeros(cnt.value, dtype=_lib.RECORD_DTYPE)
+        if cnt.value:
+            self._call(self._L.pxr_read_cluster_records, _ptr(out), cnt.value, C.byref(cnt))
+        return out
+
     def set_stream(self, stream_ptr: int | None) -> None:
         self._call(self._L.pxr_set_stream, C.c_void_p(stream_ptr) if stream_ptr else None)
 
