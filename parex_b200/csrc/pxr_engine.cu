@@ -143,7 +143,7 @@ __global__ void k_refresh_scaled(const float* x, const uint32_t* ideg, uint32_t 
 // == 2m, non-decreasing offsets, columns < n; also the maximum row length.
 template <typename OffT>
 __global__ void k_validate(const OffT* off, const uint32_t* cols, uint32_t n, uint64_t slots, uint32_t* bad,
-                           uint32_t* maxdeg, uint32_t* heavy, uint32_t* n_heavy) {
+                           uint32_t* maxdeg) {
     uint32_t b = 0, mx = 0;
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -153,7 +153,6 @@ __global__ void k_validate(const OffT* off, const uint32_t* cols, uint32_t n, ui
         else {
             const uint64_t len = (uint64_t)(z - a);
             mx = max(mx, (uint32_t)min(len, (uint64_t)0xFFFFFFFFu));
-            if (len > kHeavyRow) heavy[atomicAdd(n_heavy, 1u)] = (uint32_t)v;   // list order is irrelevant
         }
     }
     if (tid == 0 && ((uint64_t)off[0] != 0 || (uint64_t)off[n] != slots)) b |= 2u;
@@ -166,6 +165,20 @@ __global__ void k_validate(const OffT* off, const uint32_t* cols, uint32_t n, ui
     if ((threadIdx.x & 31u) == 0) {
         if (b) atomicOr(bad, b);
         if (mx) atomicMax(maxdeg, mx);
+    }
+}
+
+// Static row bins: rows longer than light_max slots go to the wide list (up
+// to wide_max slots, a warp each) or the heavy list (a CTA each); the order
+// inside a list is irrelevant.
+template <typename OffT>
+__global__ void k_bin_rows(const OffT* off, uint32_t n, uint32_t light_max, uint32_t wide_max, uint32_t* wide,
+                           uint32_t* heavy, uint32_t* counts) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint64_t len = (uint64_t)(off[v + 1] - off[v]);
+        if (len <= light_max) continue;
+        if (len <= wide_max) wide[atomicAdd(&counts[0], 1u)] = v;
+        else heavy[atomicAdd(&counts[1], 1u)] = v;
     }
 }
 
@@ -247,7 +260,11 @@ struct pxr_handle {
     RoundCtr* h_ctr = nullptr;  // pinned mirror
 
     uint32_t* d_check = nullptr;   // [3]: invalid-input bits, max row length, heavy rows
-    uint32_t* heavy = nullptr;     // vertices with more than kHeavyRow slots
+    uint32_t light_max = kLightRow;   // row bins (see k_bin_rows)
+    uint32_t wide_max = kWideRow;
+    uint32_t* wide = nullptr;
+    uint32_t n_wide = 0;
+    uint32_t* heavy = nullptr;
     uint32_t n_heavy = 0;
     // learned sweep schedule
     pxr_schedule sched{};
@@ -357,6 +374,9 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.sort = h->sort;
     d.sort_end_bit = h->sort_end_bit;
     d.root_end_bit = h->root_end_bit;
+    d.light_max = h->light_max;
+    d.wide = h->wide;
+    d.n_wide = h->n_wide;
     d.heavy = h->heavy;
     d.n_heavy = h->n_heavy;
     d.sched = h->sched.mode;
@@ -421,6 +441,16 @@ void collect_phases(pxr_handle* h) {
 // ---------------------------------------------------------------------------
 // stages
 
+// launches of the long-row kernels: warp per wide row, CTA per heavy row
+int long_launches(const pxr_handle* h) { return (h->n_wide ? 1 : 0) + (h->n_heavy ? 1 : 0); }
+uint32_t wide_grid(const pxr_handle* h) { return std::min((h->n_wide + kBlock / 32 - 1) / (kBlock / 32), 148u * 16u); }
+uint32_t heavy_grid(const pxr_handle* h) { return std::min(h->n_heavy, 148u * 16u); }
+#define PXR_LONG(h, kern, ...)                                                                         \
+    do {                                                                                               \
+        if ((h)->n_wide) kern<OffT, 32><<<wide_grid(h), kBlock, 0, s>>>(__VA_ARGS__);                 \
+        if ((h)->n_heavy) kern<OffT, kBlock><<<heavy_grid(h), kBlock, 0, s>>>(__VA_ARGS__);           \
+    } while (0)
+
 void hold_for_profiling(pxr_handle* h) {
     if (h->profiling) k_hold<<<1, 1, 0, h->stream>>>(300000u);
 }
@@ -431,11 +461,10 @@ cudaError_t op_walk(pxr_handle* h) {
     cudaStream_t s = h->stream;
     hold_for_profiling(h);
     phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
-    const uint32_t hgrid = std::min(h->n_heavy, 148u * 16u);
-    phase(h, kPhWalk, h->n_heavy ? 2 : 1, [&] {
+    phase(h, kPhWalk, 1 + long_launches(h), [&] {
         k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
                                                                           h->xt[h->xcur ^ 1]);
-        if (h->n_heavy) k_walk_heavy<OffT><<<hgrid, kBlock, 0, s>>>(d, h->xt[h->xcur], h->xt[h->xcur ^ 1]);
+        PXR_LONG(h, k_walk_long, d, h->xt[h->xcur], h->xt[h->xcur ^ 1]);
     });
     phase(h, kPhBook, 1, [&] { k_after_walk<OffT><<<1, 1, 0, s>>>(d); });
     h->xcur ^= 1;
@@ -452,9 +481,9 @@ cudaError_t op_sweep(pxr_handle* h) {
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     if (h->sched.mode)
         phase(h, kPhSched, 1, [&] { k_due_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t); });
-    phase(h, kPhNodeDiff, h->n_heavy ? 2 : 1, [&] {
+    phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
         k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
-        if (h->n_heavy) k_nodediff_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d);
+        PXR_LONG(h, k_nodediff_long, d);
     });
     phase(h, kPhEmit, 1, [&] {
         if (h->sched.mode)
@@ -493,12 +522,12 @@ cudaError_t op_cut(pxr_handle* h) {
     phase(h, kPhCutInit, 1, [&] {
         k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });
-    phase(h, kPhUnion, h->n_heavy ? 4 : 3, [&] {
+    phase(h, kPhUnion, 3 + long_launches(h), [&] {
         k_link_first<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
         k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
         k_union<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0],
                                                                            h->keys[1]);
-        if (h->n_heavy) k_union_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d);
+        PXR_LONG(h, k_union_long, d);
     });
     phase(h, kPhComponents, 1, [&] {
         k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1],
@@ -526,10 +555,9 @@ cudaError_t op_cut(pxr_handle* h) {
         k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
                                                h->act[h->acur ^ 1]);
     });
-    phase(h, kPhDisable, h->n_heavy ? 2 : 1, [&] {
+    phase(h, kPhDisable, 1 + long_launches(h), [&] {
         k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
-        if (h->n_heavy)
-            k_disable_heavy<OffT><<<std::min(h->n_heavy, 148u * 16u), kBlock, 0, s>>>(d, h->xt[h->xcur], nt);
+        PXR_LONG(h, k_disable_long, d, h->xt[h->xcur], nt);
     });
     phase(h, kPhCvol, 1, [&] { k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt); });
     if (h->sched.mode || d.trace)
@@ -742,7 +770,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->sort.pass_info, kMaxPasses + 1); A(&h->sort.tile_ctr, kMaxPasses); A(&h->sort.epoch, 1);
     A(&h->sort.status, (size_t)sort_tiles * kRadix);
     A(&h->sort_end_bit, 1); A(&h->root_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
-    A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 4); A(&h->heavy, N);
+    A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 4); A(&h->heavy, N); A(&h->wide, N);
 #undef A
     if (e != cudaSuccess) { release(h); return cuda_fail(h, e, "cudaMalloc"); }
     h->sort.max_tiles = sort_tiles;
@@ -764,6 +792,34 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     PXR_CUDA(h, cudaMemcpyAsync(h->root_end_bit, &consts[0], 4, cudaMemcpyHostToDevice, s));
     PXR_CUDA(h, cudaMemcpyAsync(h->fp_end_bit, &consts[1], 4, cudaMemcpyHostToDevice, s));
     PXR_CUDA(h, cudaMemcpyAsync(h->d_n, &consts[2], 4, cudaMemcpyHostToDevice, s));
+    return PXR_OK;
+}
+
+// Lanes per light row and the row-bin bounds.
+struct RowPlan {
+    uint32_t W, light_max, wide_max;
+};
+
+// Without tuning: one thread per row for sparse graphs (4 independent slots
+// per step), more lanes as the mean degree grows.
+RowPlan default_row_plan(const pxr_handle* h, uint32_t n, uint64_t m) {
+    (void)h;
+    const double mean = n ? (double)(2 * m) / n : 0.0;
+    const uint32_t W = mean <= 16.0 ? 1u : mean <= 32.0 ? 4u : mean <= 64.0 ? 8u : 32u;
+    return RowPlan{W, kLightRow, kWideRow};
+}
+
+template <typename OffT>
+pxr_status bin_rows(pxr_handle* h, const RowPlan& p, uint32_t* counts) {
+    cudaStream_t s = h->stream;
+    PXR_CUDA(h, cudaMemsetAsync(&h->d_check[2], 0, 8, s));
+    if (h->n) {
+        k_bin_rows<OffT><<<grid_for(h->n), kBlock, 0, s>>>(static_cast<const OffT*>(h->off), h->n, p.light_max,
+                                                           p.wide_max, h->wide, h->heavy, &h->d_check[2]);
+        ++h->launches;
+    }
+    PXR_CUDA(h, cudaMemcpyAsync(counts, &h->d_check[2], 8, cudaMemcpyDeviceToHost, s));
+    PXR_CUDA(h, cudaStreamSynchronize(s));
     return PXR_OK;
 }
 
@@ -790,8 +846,7 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     if (m) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, kind, s));
     PXR_CUDA(h, cudaMemsetAsync(h->d_check, 0, 16, s));
     k_validate<OffT><<<grid_for(std::max<uint64_t>(h->slots, n)), kBlock, 0, s>>>(
-        static_cast<const OffT*>(h->off), h->cols, n, h->slots, &h->d_check[0], &h->d_check[1], h->heavy,
-        &h->d_check[2]);
+        static_cast<const OffT*>(h->off), h->cols, n, h->slots, &h->d_check[0], &h->d_check[1]);
     ++h->launches;
     uint32_t check[4] = {0, 0, 0, 0};
     PXR_CUDA(h, cudaMemcpyAsync(check, h->d_check, 16, cudaMemcpyDeviceToHost, s));
@@ -800,17 +855,21 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     if (check[0] & 1u) return fail(h, PXR_INVALID_ARG, "offsets must be non-decreasing");
     if (check[0] & 4u) return fail(h, PXR_INVALID_ARG, "column index out of range");
     h->maxdeg = check[1];
-    const uint32_t n_heavy = check[2];
     const uint32_t nb_bits = host_bitlen(std::max<uint64_t>(n, h->maxdeg));
-    // lanes per vertex: one thread per row for sparse graphs (4 independent
-    // slots per step), more lanes as the mean degree grows
-    const double mean = n ? (double)(2 * m) / n : 0.0;
-    const uint32_t W = mean <= 16.0 ? 1u : mean <= 32.0 ? 4u : mean <= 64.0 ? 8u : 32u;
-    // captured round graphs bake in buffers, nb_bits and W: keep them only if all are unchanged
-    if (!reuse || nb_bits != h->nb_bits || W != h->W || n_heavy != h->n_heavy) drop_graphs(h);
+    RowPlan plan = default_row_plan(h, n, m);
+    uint32_t bins[2] = {0, 0};
+    pxr_status bst = bin_rows<OffT>(h, plan, bins);
+    if (bst != PXR_OK) return bst;
+    // captured round graphs bake in buffers, nb_bits and the row plan: keep them only if all are unchanged
+    if (!reuse || nb_bits != h->nb_bits || plan.W != h->W || plan.light_max != h->light_max ||
+        plan.wide_max != h->wide_max || bins[0] != h->n_wide || bins[1] != h->n_heavy)
+        drop_graphs(h);
     h->nb_bits = nb_bits;
-    h->W = W;
-    h->n_heavy = n_heavy;
+    h->W = plan.W;
+    h->light_max = plan.light_max;
+    h->wide_max = plan.wide_max;
+    h->n_wide = bins[0];
+    h->n_heavy = bins[1];
     // round state: one cluster, every vertex active; keep the growing epochs
     RoundCtr c;
     PXR_CUDA(h, cudaMemcpyAsync(&c, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, s));

@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
         const bool valid = j < count;
         uint32_t v = valid ? ids[j] : 0u;
         OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
-        const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
-        if (!light) beg = end;      // heavy rows: k_walk_heavy
+        const bool light = valid && (uint64_t)(end - beg) <= d.light_max;
+        if (!light) beg = end;      // long rows: k_walk_long
         int64_t acc = 0;
         for (OffT s = beg + gl; s < end; s += 4 * W) {
             uint32_t nb[4];
@@ -266,8 +266,8 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
         if (!in) v = 0u;
         const uint32_t mine = in ? ordered_bits(d.x[v]) : 0u;
         OffT beg = in ? d.off[v] : 0, end = in ? d.off[v + 1] : 0;
-        const bool light = in && (uint64_t)(end - beg) <= kHeavyRow;
-        if (!light) beg = end;      // heavy rows: k_nodediff_heavy
+        const bool light = in && (uint64_t)(end - beg) <= d.light_max;
+        if (!light) beg = end;      // long rows: k_nodediff_long
         int32_t c = 0;
         for (OffT s = beg + gl; s < end; s += 4 * W) {
             uint32_t nb[4];
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTabl
         const uint32_t cuts_in_warp = __ballot_sync(__activemask(), cut);
         if (cut && (cuts_in_warp & lanemask_lt()) == 0u) atomicAdd(&d.ctr->n_cut, (uint32_t)__popc(cuts_in_warp));
         if (!acted && swept && sp < d.sc_threshold) atomicAdd(&d.ctr->stat_false_stops, 1ull);
-        if (acted && !split && (d.sched || d.trace)) d.rootc[t.root[c]] = (kOriginSwept << 30) | c;
+        if (acted && !split) d.rootc[t.root[c]] = (kOriginSwept << 30) | c;
         if (acted && !split) {
             const uint32_t r = t.root[c];
             d.acc_max[r] = 0u;
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* v
         const uint32_t v = vals[j];
         const int32_t lv = d.lab[v];
         const OffT beg = d.off[v], end = d.off[v + 1];
-        if ((uint64_t)(end - beg) > kHeavyRow) continue;   // k_union_heavy
+        if ((uint64_t)(end - beg) > d.light_max) continue;   // k_union_long
         for (OffT s = beg + gl; s < end; s += W) {
             const uint32_t nb = d.cols[s];
             if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
@@ -581,7 +581,7 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
                 atomicMin(&d.parent[v], r);
                 if (r == v) {
                     my_roots[n_my++] = r;
-                    if (d.sched || d.trace) d.rootc[r] = (kOriginChild << 30) | c;
+                    d.rootc[r] = (kOriginChild << 30) | c;
                 }
             } else {
                 r = t.root[c];
@@ -685,18 +685,17 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
             nt.start[nl] = (uint32_t)(p >> 32);
             nt.root[nl] = r;
             nt.best[nl] = ~0ull;
-            nt.vol[nl] = 0u;
-            if (d.sched) {
-                const uint32_t info = d.rootc[r];
-                const bool carried = (info >> 30) == kOriginCarried;
-                d.nflag[nl] = carried ? 1u : 0u;
-                if (carried) {
-                    const uint32_t c = info & kOriginLabelMask;
-                    nt.vol[nl] = t.vol[c];
-                    const uint16_t sk = t.skip[c];
-                    nt.skip[nl] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
-                    nt.hist[nl] = t.hist[c];
-                }
+            // a cluster that was not split keeps its rows, degrees and volume:
+            // only the clusters born from a split rescan their rows
+            const uint32_t info = d.rootc[r];
+            const uint32_t kind = info >> 30;
+            const uint32_t c = info & kOriginLabelMask;
+            d.nflag[nl] = kind == kOriginCarried ? kRowsCarried : kind == kOriginSwept ? kRowsKept : kRowsScan;
+            nt.vol[nl] = kind == kOriginChild ? 0u : t.vol[c];
+            if (kind == kOriginCarried) {
+                const uint16_t sk = t.skip[c];
+                nt.skip[nl] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+                nt.hist[nl] = t.hist[c];
             }
         } else {
             const int32_t nl = (int32_t)((uint32_t)smallest - j - 1u);
@@ -823,10 +822,11 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         const bool valid = q < nkept;
         const uint32_t v = valid ? s_list[q] : 0u;
         const int32_t lv = valid ? d.lab[v] : 0;
-        const bool carried = valid && d.sched && d.nflag[lv];   // rows, degree and x/d unchanged
+        const uint32_t rows = valid ? d.nflag[lv] : kRowsScan;
+        const bool noscan = rows != kRowsScan;   // not split: no slot can have become inter-cluster
         OffT beg = valid ? d.off[v] : 0, end = valid ? d.off[v + 1] : 0;
-        const bool light = valid && (uint64_t)(end - beg) <= kHeavyRow;
-        if (!light || carried) beg = end;      // heavy rows: k_disable_heavy
+        const bool light = valid && (uint64_t)(end - beg) <= d.light_max;
+        if (!light || noscan) beg = end;      // long rows: k_disable_long
         uint32_t deg = 0;
         for (OffT s = beg + gl; s < end; s += 4 * W) {
             uint32_t nb[4];
@@ -844,11 +844,16 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         }
 #pragma unroll
         for (int o = W / 2; o > 0; o >>= 1) deg += __shfl_xor_sync(0xFFFFFFFFu, deg, o, W);
-        if (valid && carried && gl == 0) {
-            const uint32_t b = __float_as_uint(fabsf(d.x[v]));
+        if (valid && noscan && gl == 0) {
+            const float xv = d.x[v];
+            if (rows == kRowsKept) {   // recentred: refresh x / degree
+                const uint32_t dg = d.ideg[v];
+                xt[v] = dg ? __double2float_rn(__ddiv_rn((double)xv, (double)dg)) : 0.0f;
+            }
+            const uint32_t b = __float_as_uint(fabsf(xv));
             vmax = b > vmax ? b : vmax;
         }
-        if (light && !carried && gl == 0) {
+        if (light && !noscan && gl == 0) {
             d.ideg[v] = deg;
             const float xv = d.x[v];
             xt[v] = deg ? __double2float_rn(__ddiv_rn((double)xv, (double)deg)) : 0.0f;
@@ -871,10 +876,12 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
 }
 
 // ---------------------------------------------------------------------------
-// Heavy rows (> kHeavyRow slots): one CTA per vertex of the static heavy
-// list, kBlock threads over the row, block reduction.  Every accumulation is
-// order-independent, so the split between these and the lane-per-row kernels
-// does not change any result.
+// Long rows.  Rows longer than Dev::light_max slots are binned once per graph
+// into two static lists: "wide" rows (up to Dev::wide_max slots) get one warp
+// each, "heavy" rows one CTA each (G = 32 or kBlock lanes per row, slots
+// strided by G with four independent loads per step, group reduction).
+// Every accumulation is order-independent, so the binning does not change
+// any result.
 
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* sh) {
@@ -890,57 +897,115 @@ __device__ __forceinline__ T block_sum(T v, T* sh) {
     return t;  // valid in thread 0
 }
 
+// sum over the G lanes of a row group; valid in the group's first lane
+template <int G, typename T>
+__device__ __forceinline__ T group_sum(T v, T* sh) {
+    if constexpr (G == 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        return v;
+    } else {
+        return block_sum<T>(v, sh);
+    }
+}
+
+// the rows of one list that a group visits: group index, group count, lane
+template <int G>
+struct RowGroups {
+    uint32_t first, step, lane;
+    __device__ __forceinline__ RowGroups() {
+        if constexpr (G == 32) {
+            first = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            step = (gridDim.x * blockDim.x) >> 5;
+            lane = threadIdx.x & 31u;
+        } else {
+            first = blockIdx.x;
+            step = gridDim.x;
+            lane = threadIdx.x;
+        }
+    }
+};
+
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_walk_heavy(Dev<OffT> d, const float* xt_in, float* xt_out) {
+__device__ __forceinline__ const uint32_t* row_list(const Dev<OffT>& d, int G, uint32_t* count) {
+    *count = G == 32 ? d.n_wide : d.n_heavy;
+    return G == 32 ? d.wide : d.heavy;
+}
+
+template <typename OffT, int G>
+__global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* xt_in, float* xt_out) {
     __shared__ int64_t sh[kBlock / 32];
-    __shared__ unsigned long long sh2[kBlock / 32];
     const int e = fixed_exponent(d.ctr->xmax_bits, d.nb_bits);
     const double scale = pow2(e), inv = pow2(-e);
-    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
-        const uint32_t v = d.heavy[h];
+    uint32_t cnt;
+    const uint32_t* list = row_list(d, G, &cnt);
+    const RowGroups<G> rg;
+    uint32_t vmax = 0;
+    unsigned long long st_v = 0, st_s = 0, st_g = 0;
+    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
+        const uint32_t v = list[h];
         if (d.lab[v] < 0) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
         int64_t acc = 0;
         unsigned long long g = 0;
-        for (OffT s = beg + threadIdx.x; s < end; s += 4 * kBlock) {
+        for (OffT s = beg + rg.lane; s < end; s += 4 * G) {
             uint32_t nb[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * kBlock < end ? d.cols[s + u * kBlock] : kInvalidEdge;
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
 #pragma unroll
             for (int u = 0; u < 4; ++u)
                 if (nb[u] != kInvalidEdge) { acc += to_fixed(xt_in[nb[u]], scale); ++g; }
         }
-        acc = block_sum<int64_t>(acc, sh);
-        g = block_sum<unsigned long long>(g, sh2);
-        if (threadIdx.x == 0) {
+        acc = group_sum<G, int64_t>(acc, sh);
+        st_g += g;
+        if (rg.lane == 0) {
             const double sum = __dmul_rn(__ll2double_rn(acc), inv);
             const double val = __dadd_rn(__dmul_rn(sum, 0.9), __dmul_rn((double)d.x[v], 0.1));
             const float xv = __double2float_rn(val);
             d.x[v] = xv;
             const uint32_t dg = d.ideg[v];
             xt_out[v] = dg ? __double2float_rn(__ddiv_rn((double)xv, (double)dg)) : 0.0f;
-            atomicMax(&d.ctr->xmax_walk_bits, __float_as_uint(fabsf(xv)));
-            atomicAdd(&d.ctr->stat_walk_vertices, 1ull);
-            atomicAdd(&d.ctr->stat_walk_slots, (unsigned long long)(end - beg));
-            atomicAdd(&d.ctr->stat_walk_gathers, g);
+            const uint32_t b = __float_as_uint(fabsf(xv));
+            vmax = b > vmax ? b : vmax;
+            st_v += 1;
+            st_s += (unsigned long long)(end - beg);
         }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+        st_v += __shfl_xor_sync(0xFFFFFFFFu, st_v, o);
+        st_s += __shfl_xor_sync(0xFFFFFFFFu, st_s, o);
+        st_g += __shfl_xor_sync(0xFFFFFFFFu, st_g, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
+        if (st_v) {
+            atomicAdd(&d.ctr->stat_walk_vertices, st_v);
+            atomicAdd(&d.ctr->stat_walk_slots, st_s);
+        }
+        if (st_g) atomicAdd(&d.ctr->stat_walk_gathers, st_g);
     }
 }
 
-template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_nodediff_heavy(Dev<OffT> d) {
+template <typename OffT, int G>
+__global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
     __shared__ int32_t sh[kBlock / 32];
-    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
-        const uint32_t v = d.heavy[h];
-        if (d.lab[v] < 0) continue;
-        if (d.sched && !(d.sflag[d.lab[v]] & 2u)) continue;
+    uint32_t cnt;
+    const uint32_t* list = row_list(d, G, &cnt);
+    const RowGroups<G> rg;
+    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
+        const uint32_t v = list[h];
+        const int32_t lv = d.lab[v];
+        if (lv < 0) continue;
+        if (d.sched && !(d.sflag[lv] & 2u)) continue;
         const uint32_t mine = ordered_bits(d.x[v]);
         const OffT beg = d.off[v], end = d.off[v + 1];
         int32_t c = 0;
-        for (OffT s = beg + threadIdx.x; s < end; s += 4 * kBlock) {
+        for (OffT s = beg + rg.lane; s < end; s += 4 * G) {
             uint32_t nb[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * kBlock < end ? d.cols[s + u * kBlock] : kInvalidEdge;
+            for (int u = 0; u < 4; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 if (nb[u] == kInvalidEdge) continue;
@@ -948,22 +1013,25 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_heavy(Dev<OffT> d) {
                 c += (o < mine || (o == mine && nb[u] < v)) ? -1 : 1;
             }
         }
-        c = block_sum<int32_t>(c, sh);
-        if (threadIdx.x == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
+        c = group_sum<G, int32_t>(c, sh);
+        if (rg.lane == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
     }
 }
 
-template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_union_heavy(Dev<OffT> d) {
+template <typename OffT, int G>
+__global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
     const uint32_t k = d.ctr->n_clusters;
-    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
-        const uint32_t v = d.heavy[h];
+    uint32_t cnt;
+    const uint32_t* list = row_list(d, G, &cnt);
+    const RowGroups<G> rg;
+    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
+        const uint32_t v = list[h];
         const int32_t lv = d.lab[v];
         if (lv < 0) continue;
         const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;   // cut labels are c or K + c
         if (c >= k || !d.split[c]) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
-        for (OffT s = beg + threadIdx.x; s < end; s += kBlock) {
+        for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
             if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
             uint32_t a = v, b = nb;
@@ -980,34 +1048,39 @@ __global__ void __launch_bounds__(kBlock) k_union_heavy(Dev<OffT> d) {
     }
 }
 
-template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_disable_heavy(Dev<OffT> d, float* xt, ClusterTables nt) {
+template <typename OffT, int G>
+__global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt, ClusterTables nt) {
     __shared__ uint32_t sh[kBlock / 32];
-    for (uint32_t h = blockIdx.x; h < d.n_heavy; h += gridDim.x) {
-        const uint32_t v = d.heavy[h];
+    uint32_t cnt;
+    const uint32_t* list = row_list(d, G, &cnt);
+    const RowGroups<G> rg;
+    uint32_t vmax = 0;
+    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
+        const uint32_t v = list[h];
         const int32_t lv = d.lab[v];
         if (lv < 0) continue;
-        if (d.sched && d.nflag[lv]) {   // carried: only its |x| counts
-            if (threadIdx.x == 0) atomicMax(&d.ctr->xmax_bits, __float_as_uint(fabsf(d.x[v])));
-            continue;
-        }
+        if (d.nflag[lv] != kRowsScan) continue;   // not split: k_ids_disable refreshed x / degree
         const OffT beg = d.off[v], end = d.off[v + 1];
         uint32_t deg = 0;
-        for (OffT s = beg + threadIdx.x; s < end; s += kBlock) {
+        for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
             if (nb == kInvalidEdge) continue;
             if (d.lab[nb] != lv) d.cols[s] = kInvalidEdge;
             else ++deg;
         }
-        deg = block_sum<uint32_t>(deg, sh);
-        if (threadIdx.x == 0) {
+        deg = group_sum<G, uint32_t>(deg, sh);
+        if (rg.lane == 0) {
             d.ideg[v] = deg;
             const float xv = d.x[v];
             xt[v] = deg ? __double2float_rn(__ddiv_rn((double)xv, (double)deg)) : 0.0f;
-            atomicMax(&d.ctr->xmax_bits, __float_as_uint(fabsf(xv)));
+            const uint32_t b = __float_as_uint(fabsf(xv));
+            vmax = b > vmax ? b : vmax;
             atomicAdd(&nt.vol[lv], deg);
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+    if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(&d.ctr->xmax_bits, vmax);
 }
 
 // exclusive prefix of cluster volumes over labels

@@ -51,6 +51,12 @@ struct ClusterTables {
 enum : uint32_t { kOriginSwept = 1u, kOriginChild = 2u, kOriginCarried = 3u };
 constexpr uint32_t kOriginLabelMask = 0x3FFFFFFFu;
 
+// What the end of a round does with the rows of a cluster (Dev::nflag):
+// a cluster born from a split rescans its rows (disables the slots that now
+// cross clusters, recounts degrees); one swept but not split keeps its rows
+// and only refreshes x / degree after recentring; a carried one is unchanged.
+enum : uint8_t { kRowsScan = 0, kRowsKept = 1, kRowsCarried = 2 };
+
 template <typename OffT>
 struct Dev {
     // graph
@@ -89,13 +95,16 @@ struct Dev {
     SortState sort;
     uint32_t* sort_end_bit;   // main sort bits
     uint32_t* root_end_bit;   // root sort bits
-    const uint32_t* heavy;    // vertices whose row exceeds kHeavyRow slots (one CTA each)
+    uint32_t light_max;       // rows up to this many slots: W lanes per row in the round kernels
+    const uint32_t* wide;     // vertices with light_max < row <= wide_max slots (one warp each)
+    uint32_t n_wide;
+    const uint32_t* heavy;    // vertices with longer rows (one CTA each)
     uint32_t n_heavy;
     // learned sweep schedule (all zero / null in the plain form)
     uint32_t sched;           // PXR_SCHEDULE_*
     uint32_t trace;           // write per-cluster records each round
     uint8_t* sflag;           // per label this round: bit 0 acted on (due), bit 1 in the sweep
-    uint8_t* nflag;           // per label of the next round: 1 when carried unswept
+    uint8_t* nflag;           // per label of the next round: kRows* (rows to rescan or not)
     uint32_t* rootc;          // per root vertex: kind << 30 | old label
     LookbackState lb_sched, lb_emit, lb_carry;
     const float* mlp;         // bf16 weights widened to float, then input mean and scale
@@ -104,9 +113,10 @@ struct Dev {
     void* records;            // pxr_cluster_record[] when trace is on
 };
 
-// Rows longer than this are processed by a whole CTA in the *_heavy kernels
-// and skipped by the lane-per-row kernels.
-constexpr uint32_t kHeavyRow = 64;
+// Default row bins: rows up to kLightRow slots go W lanes per row, up to
+// kWideRow a warp per row, longer rows a CTA per row.
+constexpr uint32_t kLightRow = 64;
+constexpr uint32_t kWideRow = 4096;
 
 // look-back sites (index into Dev::lb_epoch and RoundCtr::tile_counter)
 enum : int {

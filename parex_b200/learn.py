@@ -248,7 +248,6 @@ def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, ma
     for _ in range(reps):
         dm.initialize(graph)
         torch.cuda.synchronize(device)
-        t0 = time.perf_counter()
         rounds = dm.expanderDecomposition()
         times.append(dm.stats()["last_decompose_ms"])
     fp = dm.getFinalPartition()
@@ -259,7 +258,7 @@ def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, ma
             "false_stops": st["false_stops"], "ids": fp.clusterIds}
 
 
-def compare(graph, model: Model, seed: int = 6582, safety: float = 0.5, max_skip: int = 16, device: int = 0,
+def compare(graph, model: Model, seed: int = 6582, safety: float = 0.25, max_skip: int = 16, device: int = 0,
             reps: int = 3, audit: bool = True) -> dict:
     plain = run_mode(graph, _lib.SCHEDULE_PLAIN, None, seed, safety, max_skip, device, reps)
     learned = run_mode(graph, _lib.SCHEDULE_LEARNED, model, seed, safety, max_skip, device, reps)
@@ -301,10 +300,12 @@ def main(argv=None) -> int:
     t.add_argument("--lr", type=float, default=3e-3)
     t.add_argument("--over", type=float, default=4.0)
     t.add_argument("--eval", action="store_true")
+    t.add_argument("--safety", type=float, nargs="*", default=[0.25])
+    t.add_argument("--max-skip", type=int, default=16)
     t.add_argument("--report", default=None)
     e = sub.add_parser("eval")
     e.add_argument("--model", default=DEFAULT_MODEL)
-    e.add_argument("--safety", type=float, nargs="*", default=[0.5])
+    e.add_argument("--safety", type=float, nargs="*", default=[0.25])
     e.add_argument("--max-skip", type=int, default=16)
     e.add_argument("--report", default=None)
     args = ap.parse_args(argv)
@@ -325,7 +326,8 @@ def main(argv=None) -> int:
         model.save(args.out)
         report["train"] = model.meta
         if args.eval:
-            report["eval"] = [compare(make(), model, seed=seed) for _, make, seed in EVAL_GRAPHS]
+            report["eval"] = [compare(make(), model, seed=seed, safety=sf, max_skip=args.max_skip)
+                              for _, make, seed in EVAL_GRAPHS for sf in args.safety]
     else:
         model = Model.load(args.model)
         report["eval"] = [compare(make(), model, seed=seed, safety=sf, max_skip=args.max_skip)
