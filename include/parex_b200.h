@@ -55,8 +55,33 @@ typedef struct {
     int32_t device;          /* CUDA device ordinal                                       */
     uint32_t division;       /* PXR_DIV_*                                                 */
     uint32_t driver;         /* PXR_DRIVER_*                                              */
-    uint32_t reserved[9];
+    uint32_t tune;           /* PXR_TUNE_* (row plan: lanes per row and row bins)          */
+    uint32_t reserved[8];
 } pxr_config;
+
+/* How the row plan of a graph is chosen (no counterpart in the reference,
+ * whose kernels use one warp per vertex for every row). */
+enum {
+    PXR_TUNE_AUTO = 0,       /* time the walk step under each candidate plan on the graph
+                                itself at initialisation, keep the fastest; the choice is
+                                cached per degree histogram for the life of the process   */
+    PXR_TUNE_HEURISTIC = 1   /* lanes per row from the mean degree, default bins           */
+};
+
+/* Row plan: rows of at most light_max slots are handled by lanes_per_row
+ * lanes each (1, 4, 8, 16 or 32; 4 slot loads in flight per lane), rows up
+ * to wide_max slots by a warp each, longer rows by a 256-thread CTA each.
+ * The plan changes speed only: every result is the same under any plan. */
+typedef struct {
+    uint32_t lanes_per_row;
+    uint32_t light_max;
+    uint32_t wide_max;
+    uint32_t wide_rows;      /* rows in the warp-per-row bin (set by the library)            */
+    uint32_t heavy_rows;     /* rows in the CTA-per-row bin (set by the library)             */
+    uint32_t source;         /* 0 heuristic, 1 tuned now, 2 tuned earlier (cache), 3 forced   */
+    uint32_t candidates;     /* plans timed by the last tuning                               */
+    float walk_us;           /* walk-step time of the chosen plan when tuned (microseconds)  */
+} pxr_row_plan;
 
 /* One sweep cut per active cluster: SweepCutData, lib/core/definitions.h:57-61. */
 typedef struct { int32_t label; float sparsity; uint32_t offset; } pxr_sweep_cut;
@@ -199,6 +224,13 @@ pxr_status pxr_initialize_device(pxr_handle* h, uint32_t n, uint64_t m,
 pxr_status pxr_initialize_batched(pxr_handle* h, uint32_t n, uint64_t m,
                                   const uint64_t* offsets, const uint32_t* cols,
                                   uint32_t n_instances, const uint32_t* instance_start);
+
+/* The row plan in use (pxr_row_plan).  No counterpart in the reference. */
+pxr_status pxr_get_row_plan(pxr_handle* h, pxr_row_plan* out);
+/* Force a row plan (lanes_per_row, light_max, wide_max are read; the rest is
+ * ignored) for this and later initialisations; NULL returns to cfg.tune.
+ * Applied at once when a graph is loaded. */
+pxr_status pxr_set_row_plan(pxr_handle* h, const pxr_row_plan* plan);
 
 /* CudaDeviceManager::iterateRandomWalk() (cuda/interface.h:29). */
 pxr_status pxr_walk_step(pxr_handle* h);

@@ -31,7 +31,7 @@ SYMBOLS = [
     "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
     "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
-    "pxr_mlp_adam_step",
+    "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -39,7 +39,16 @@ STATIC_SCRATCH_MAX_LABELS = 65536
 class Config(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("sc_threshold", C.c_float), ("rw_threshold", C.c_float),
                 ("max_rounds", C.c_uint32), ("device", C.c_int32), ("division", C.c_uint32),
-                ("driver", C.c_uint32), ("reserved", C.c_uint32 * 9)]
+                ("driver", C.c_uint32), ("tune", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+
+
+TUNE_AUTO, TUNE_HEURISTIC = 0, 1
+
+
+class RowPlan(C.Structure):
+    _fields_ = [("lanes_per_row", C.c_uint32), ("light_max", C.c_uint32), ("wide_max", C.c_uint32),
+                ("wide_rows", C.c_uint32), ("heavy_rows", C.c_uint32), ("source", C.c_uint32),
+                ("candidates", C.c_uint32), ("walk_us", C.c_float)]
 
 
 class SweepCut(C.Structure):
@@ -152,6 +161,8 @@ def load() -> C.CDLL:
     L.pxr_set_state.argtypes = [p, p, p, u32, p, p, p, u32, i32, C.c_int]
     L.pxr_initialize_batched.argtypes = [p, u32, u64, p, p, u32, p]
     L.pxr_set_schedule.argtypes = [p, C.POINTER(Schedule), p, p]
+    L.pxr_get_row_plan.argtypes = [p, C.POINTER(RowPlan)]
+    L.pxr_set_row_plan.argtypes = [p, C.POINTER(RowPlan)]
     L.pxr_read_cluster_records.argtypes = [p, p, u32, C.POINTER(u32)]
     L.pxr_mlp_forward.argtypes = [p, u32, p, p, p, p]
     L.pxr_mlp_scratch_floats.argtypes = [u32]

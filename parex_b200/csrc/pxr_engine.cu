@@ -1,7 +1,10 @@
 // Host side of parex_b200: the handle, device memory, the round drivers and
 // the C ABI declared in include/parex_b200.h.
 #include <algorithm>
+#include <array>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -182,6 +185,22 @@ __global__ void k_bin_rows(const OffT* off, uint32_t n, uint32_t light_max, uint
     }
 }
 
+// rows per bit length of their size (0: empty rows, 32: 2^31 slots or more)
+template <typename OffT>
+__global__ void k_degree_hist(const OffT* off, uint32_t n, uint32_t* hist) {
+    __shared__ uint32_t sh[33];
+    for (int i = threadIdx.x; i < 33; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint64_t len = (uint64_t)(off[v + 1] - off[v]);
+        const uint32_t b = len >= (1ull << 31) ? 32u : (len ? 32u - __clz((uint32_t)len) : 0u);
+        atomicAdd(&sh[b], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 33; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
 // Profiling aid: hold the stream for a moment so the host can queue a whole
 // op before the device starts it; the phase events then time device work
 // rather than host launch latency.
@@ -260,10 +279,14 @@ struct pxr_handle {
     RoundCtr* h_ctr = nullptr;  // pinned mirror
 
     uint32_t* d_check = nullptr;   // [3]: invalid-input bits, max row length, heavy rows
+    RoundCtr* probe_ctr = nullptr;    // scratch counters for the tuner's timed walk steps
+    bool plan_forced = false;
+    pxr_row_plan plan_info{};         // last plan chosen (pxr_get_row_plan)
     uint32_t light_max = kLightRow;   // row bins (see k_bin_rows)
     uint32_t wide_max = kWideRow;
     uint32_t* wide = nullptr;
     uint32_t n_wide = 0;
+    uint32_t* hist = nullptr;         // [33] rows per bit length of the row size
     uint32_t* heavy = nullptr;
     uint32_t n_heavy = 0;
     // learned sweep schedule
@@ -771,6 +794,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->sort.status, (size_t)sort_tiles * kRadix);
     A(&h->sort_end_bit, 1); A(&h->root_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
     A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 4); A(&h->heavy, N); A(&h->wide, N);
+    A(&h->probe_ctr, 1); A(&h->hist, 33);
 #undef A
     if (e != cudaSuccess) { release(h); return cuda_fail(h, e, "cudaMalloc"); }
     h->sort.max_tiles = sort_tiles;
@@ -823,6 +847,161 @@ pxr_status bin_rows(pxr_handle* h, const RowPlan& p, uint32_t* counts) {
     return PXR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Row-plan autotuner: time one walk step (the light-row kernel plus the
+// warp- and CTA-per-row kernels) of the whole graph under each candidate
+// plan, on the graph's own rows and potentials, and keep the fastest.  The
+// walk writes only scratch (a copy of x, a scratch x / degree and scratch
+// counters), so the state is untouched.  Plans are cached per (n, m, offset
+// width, row-size histogram) for the life of the process.
+
+std::mutex g_plan_mu;
+std::map<std::vector<uint64_t>, RowPlan> g_plan_cache;
+
+template <typename OffT, int W>
+cudaError_t probe_walk(pxr_handle* h, Dev<OffT> d, float* xt_out) {
+    cudaStream_t s = h->stream;
+    k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur], xt_out);
+    PXR_LONG(h, k_walk_long, d, h->xt[h->xcur], xt_out);
+    return cudaGetLastError();
+}
+
+template <typename OffT>
+cudaError_t probe_walk_w(pxr_handle* h, const Dev<OffT>& d, float* xt_out) {
+    switch (h->W) {
+        case 1: return probe_walk<OffT, 1>(h, d, xt_out);
+        case 4: return probe_walk<OffT, 4>(h, d, xt_out);
+        case 16: return probe_walk<OffT, 16>(h, d, xt_out);
+        case 32: return probe_walk<OffT, 32>(h, d, xt_out);
+        default: return probe_walk<OffT, 8>(h, d, xt_out);
+    }
+}
+
+template <typename OffT>
+pxr_status tune_row_plan(pxr_handle* h, const std::array<uint32_t, 33>& hist, RowPlan* best, uint32_t* tried,
+                         float* best_us) {
+    cudaStream_t s = h->stream;
+    const uint32_t n = h->n;
+    // rows of the largest size class decide which bin bounds can differ
+    int top = 0;
+    for (int b = 0; b < 33; ++b)
+        if (hist[b]) top = b;
+    const uint64_t maxlen = top == 0 ? 0 : (1ull << top) - 1;   // upper bound of the largest class
+    std::vector<RowPlan> cands;
+    const uint32_t lanes[] = {1, 4, 8, 16, 32};
+    const uint32_t lights[] = {16, 32, 64, 128};
+    const uint32_t wides[] = {1024, 4096, 16384};
+    // a bound above the previous one that already holds every row gives the same bins: skip it
+    for (uint32_t W : lanes)
+        for (int i = 0; i < 4; ++i) {
+            if (i > 0 && (uint64_t)lights[i - 1] >= maxlen) continue;
+            for (int j = 0; j < 3; ++j) {
+                if (j > 0 && (uint64_t)wides[j - 1] >= maxlen) continue;
+                cands.push_back(RowPlan{W, lights[i], wides[j]});
+            }
+        }
+    // scratch: x copy in keys[0], x / degree in keys[1], counters in probe_ctr
+    float* xs = reinterpret_cast<float*>(h->keys[0]);
+    float* xo = reinterpret_cast<float*>(h->keys[1]);
+    PXR_CUDA(h, cudaMemcpyAsync(xs, h->x, (size_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(h->probe_ctr, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToDevice, s));
+    cudaEvent_t e0 = take_event(h), e1 = take_event(h);
+    float best_ms = 0.0f;
+    bool have = false;
+    for (const RowPlan& p : cands) {
+        uint32_t bins[2];
+        pxr_status st = bin_rows<OffT>(h, p, bins);
+        if (st != PXR_OK) return st;
+        h->W = p.W;
+        h->light_max = p.light_max;
+        h->wide_max = p.wide_max;
+        h->n_wide = bins[0];
+        h->n_heavy = bins[1];
+        Dev<OffT> d = make_dev<OffT>(h);
+        d.x = xs;
+        d.ctr = h->probe_ctr;
+        PXR_CUDA(h, probe_walk_w<OffT>(h, d, xo));     // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; ++r) PXR_CUDA(h, probe_walk_w<OffT>(h, d, xo));
+        cudaEventRecord(e1, s);
+        PXR_CUDA(h, cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        PXR_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+        h->launches += 4ull * (1 + long_launches(h));
+        if (!have || ms < best_ms) { best_ms = ms; *best = p; have = true; }
+    }
+    h->event_pool.push_back(e0);
+    h->event_pool.push_back(e1);
+    *tried = (uint32_t)cands.size();
+    *best_us = best_ms * 1000.0f / 3.0f;
+    return PXR_OK;
+}
+
+// The plan for the graph just uploaded: forced, cached, tuned or heuristic.
+// Rebins the rows and drops captured graphs when the plan changed.
+template <typename OffT>
+pxr_status choose_row_plan(pxr_handle* h, bool reuse, uint32_t nb_bits) {
+    const RowPlan old{h->W, h->light_max, h->wide_max};
+    const uint32_t old_wide = h->n_wide, old_heavy = h->n_heavy, old_bits = h->nb_bits;
+    RowPlan plan = default_row_plan(h, h->n, h->m);
+    uint32_t source = 0, tried = 0;
+    float us = 0.0f;
+    if (h->plan_forced) {
+        plan = RowPlan{h->plan_info.lanes_per_row, h->plan_info.light_max, h->plan_info.wide_max};
+        source = 3;
+    } else if (h->cfg.tune == PXR_TUNE_AUTO && h->n > 0) {
+        cudaStream_t s = h->stream;
+        std::array<uint32_t, 33> hist{};
+        PXR_CUDA(h, cudaMemsetAsync(h->hist, 0, 33 * 4, s));
+        k_degree_hist<OffT><<<std::min(grid_for(h->n), 148u * 4u), kBlock, 0, s>>>(static_cast<const OffT*>(h->off),
+                                                                                   h->n, h->hist);
+        ++h->launches;
+        PXR_CUDA(h, cudaMemcpyAsync(hist.data(), h->hist, 33 * 4, cudaMemcpyDeviceToHost, s));
+        PXR_CUDA(h, cudaStreamSynchronize(s));
+        std::vector<uint64_t> key{h->n, h->m, sizeof(OffT)};
+        key.insert(key.end(), hist.begin(), hist.end());
+        bool hit = false;
+        {
+            std::lock_guard<std::mutex> lk(g_plan_mu);
+            auto it = g_plan_cache.find(key);
+            if (it != g_plan_cache.end()) { plan = it->second; hit = true; }
+        }
+        if (hit) {
+            source = 2;
+        } else {
+            pxr_status st = tune_row_plan<OffT>(h, hist, &plan, &tried, &us);
+            if (st != PXR_OK) return st;
+            source = 1;
+            std::lock_guard<std::mutex> lk(g_plan_mu);
+            g_plan_cache[key] = plan;
+        }
+    }
+    uint32_t bins[2] = {0, 0};
+    pxr_status bst = bin_rows<OffT>(h, plan, bins);
+    if (bst != PXR_OK) return bst;
+    // captured round graphs bake in buffers, nb_bits and the row plan: keep them only if all are unchanged
+    if (!reuse || nb_bits != old_bits || plan.W != old.W || plan.light_max != old.light_max ||
+        plan.wide_max != old.wide_max || bins[0] != old_wide || bins[1] != old_heavy)
+        drop_graphs(h);
+    h->nb_bits = nb_bits;
+    h->W = plan.W;
+    h->light_max = plan.light_max;
+    h->wide_max = plan.wide_max;
+    h->n_wide = bins[0];
+    h->n_heavy = bins[1];
+    h->plan_info.lanes_per_row = plan.W;
+    h->plan_info.light_max = plan.light_max;
+    h->plan_info.wide_max = plan.wide_max;
+    h->plan_info.wide_rows = bins[0];
+    h->plan_info.heavy_rows = bins[1];
+    h->plan_info.source = source;
+    if (source == 1) {
+        h->plan_info.candidates = tried;
+        h->plan_info.walk_us = us;
+    }
+    return PXR_OK;
+}
+
 // offsets/cols: host pointers (kind = cudaMemcpyHostToDevice) or device pointers
 template <typename OffT>
 pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* offsets, const uint32_t* cols,
@@ -856,20 +1035,6 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     if (check[0] & 4u) return fail(h, PXR_INVALID_ARG, "column index out of range");
     h->maxdeg = check[1];
     const uint32_t nb_bits = host_bitlen(std::max<uint64_t>(n, h->maxdeg));
-    RowPlan plan = default_row_plan(h, n, m);
-    uint32_t bins[2] = {0, 0};
-    pxr_status bst = bin_rows<OffT>(h, plan, bins);
-    if (bst != PXR_OK) return bst;
-    // captured round graphs bake in buffers, nb_bits and the row plan: keep them only if all are unchanged
-    if (!reuse || nb_bits != h->nb_bits || plan.W != h->W || plan.light_max != h->light_max ||
-        plan.wide_max != h->wide_max || bins[0] != h->n_wide || bins[1] != h->n_heavy)
-        drop_graphs(h);
-    h->nb_bits = nb_bits;
-    h->W = plan.W;
-    h->light_max = plan.light_max;
-    h->wide_max = plan.wide_max;
-    h->n_wide = bins[0];
-    h->n_heavy = bins[1];
     // round state: one cluster, every vertex active; keep the growing epochs
     RoundCtr c;
     PXR_CUDA(h, cudaMemcpyAsync(&c, h->ctr, sizeof(RoundCtr), cudaMemcpyDeviceToHost, s));
@@ -892,6 +1057,7 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     }
     pxr_status st = setup_tables_initial(h);
     if (st == PXR_OK) st = reset_schedule_state(h);
+    if (st == PXR_OK) st = choose_row_plan<OffT>(h, reuse, nb_bits);
     if (st != PXR_OK) return st;
     PXR_CUDA(h, cudaGetLastError());
     if (batched) return PXR_OK;   // batch_setup completes the state
@@ -1435,6 +1601,32 @@ pxr_status pxr_read_cluster_records(pxr_handle* h, pxr_cluster_record* out, uint
         PXR_CUDA(h, cudaStreamSynchronize(h->stream));
     }
     return PXR_OK;
+}
+
+pxr_status pxr_get_row_plan(pxr_handle* h, pxr_row_plan* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    *out = h->plan_info;
+    return PXR_OK;
+}
+
+pxr_status pxr_set_row_plan(pxr_handle* h, const pxr_row_plan* plan) {
+    if (!h) return PXR_INVALID_ARG;
+    if (plan) {
+        const uint32_t W = plan->lanes_per_row;
+        if (!(W == 1 || W == 4 || W == 8 || W == 16 || W == 32))
+            return fail(h, PXR_INVALID_ARG, "lanes_per_row must be 1, 4, 8, 16 or 32");
+        if (plan->light_max == 0 || plan->wide_max < plan->light_max)
+            return fail(h, PXR_INVALID_ARG, "need 0 < light_max <= wide_max");
+        h->plan_info.lanes_per_row = W;
+        h->plan_info.light_max = plan->light_max;
+        h->plan_info.wide_max = plan->wide_max;
+        h->plan_forced = true;
+    } else {
+        h->plan_forced = false;
+    }
+    if (!h->initialized) return PXR_OK;
+    PXR_CUDA(h, cudaSetDevice(h->device));
+    return h->off64 ? choose_row_plan<uint64_t>(h, true, h->nb_bits) : choose_row_plan<uint32_t>(h, true, h->nb_bits);
 }
 
 }  // extern "C"

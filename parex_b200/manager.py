@@ -61,7 +61,7 @@ class CudaDeviceManager:
 
     def __init__(self, seed: int = 6582, sc_threshold: float = 0.3, rw_threshold: float = 1e-4,
                  max_rounds: int = 200000, device: int = 0, division: int = _lib.DIV_IEEE,
-                 driver: int = _lib.DRIVER_GRAPH):
+                 driver: int = _lib.DRIVER_GRAPH, tune: int = _lib.TUNE_AUTO):
         L = _lib.load()
         cfg = _lib.Config()
         L.pxr_config_default(C.byref(cfg))
@@ -72,6 +72,7 @@ class CudaDeviceManager:
         cfg.device = device
         cfg.division = division
         cfg.driver = driver
+        cfg.tune = tune
         self._h = C.c_void_p()
         _lib.check(None, L.pxr_create(C.byref(cfg), C.byref(self._h)))
         self._L = L
@@ -245,6 +246,20 @@ class CudaDeviceManager:
         if cnt.value:
             self._call(self._L.pxr_read_cluster_records, _ptr(out), cnt.value, C.byref(cnt))
         return out
+
+    def row_plan(self) -> dict:
+        """The row plan in use (pxr_get_row_plan)."""
+        rp = _lib.RowPlan()
+        self._call(self._L.pxr_get_row_plan, C.byref(rp))
+        return {f: getattr(rp, f) for f, _ in _lib.RowPlan._fields_}
+
+    def set_row_plan(self, lanes_per_row: int | None = None, light_max: int = 64, wide_max: int = 4096) -> None:
+        """Force a row plan; with no arguments return to the configured tuning."""
+        if lanes_per_row is None:
+            self._call(self._L.pxr_set_row_plan, None)
+            return
+        rp = _lib.RowPlan(lanes_per_row, light_max, wide_max)
+        self._call(self._L.pxr_set_row_plan, C.byref(rp))
 
     def set_stream(self, stream_ptr: int | None) -> None:
         self._call(self._L.pxr_set_stream, C.c_void_p(stream_ptr) if stream_ptr else None)

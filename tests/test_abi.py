@@ -40,6 +40,7 @@ def test_struct_sizes_match_header():
     assert C.sizeof(_lib.NodeData) == 16      # NodeData
     assert C.sizeof(_lib.Stats) == 104
     assert C.sizeof(_lib.Schedule) == 32
+    assert C.sizeof(_lib.RowPlan) == 32
     assert C.sizeof(_lib.ClusterRecord) == 128 == _lib.RECORD_DTYPE.itemsize
     assert C.sizeof(_lib.PhaseStat) == 40
 
