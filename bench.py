@@ -48,10 +48,33 @@ SIDE = 128
 L2_FLUSH_BYTES = 256 << 20
 
 
-def workload_config(g, extra=None):
+WORKLOADS = {
+    "grid128": "3D 7-point grid 128^3 (2,097,152 vertices, 6,242,304 edges)",
+    "sbm16k": "planted partition n=16,384, 16 blocks, intra degree 12, inter degree 0.5, seed 6582",
+    "rmat22": "R-MAT scale 22, edge factor 16, (a,b,c)=(0.57,0.19,0.19), seed 1, built on the GPU",
+    "rmat24": "R-MAT scale 24, edge factor 16, (a,b,c)=(0.57,0.19,0.19), seed 1, built on the GPU",
+    "regular22": "random 8-regular graph on 2^22 vertices, seed 1 (the no-split case)",
+}
+
+
+def load_workload(name, dev=None):
+    """(CSRGraph or None, device offsets, device cols, n, m) for a named workload."""
+    from parex_b200 import graphs as G
+    if name.startswith("rmat"):
+        import torch
+        from parex_b200 import gpu_build as B
+        off_d, cols_d, n, m = B.rmat(int(name[4:]), 16, seed=1, device=dev.index or 0)
+        return None, off_d, cols_d, n, m
+    g = {"grid128": lambda: G.grid3d(SIDE), "sbm16k": lambda: G.sbm_graph(),
+         "regular22": lambda: G.random_regular(1 << 22, 8, seed=1)}[name]()
+    return g, None, None, g.n, g.m
+
+
+def workload_config(g, extra=None, name="grid128"):
+    n, m = (g.n, g.m) if hasattr(g, "n") else g
     cfg = {
-        "workload": f"grid3d_{SIDE}: 3D 7-point grid {SIDE}^3, seed {SEED}, sc {SC}, rw {RW}",
-        "n": g.n, "m": g.m, "seed": SEED, "sc_threshold": SC, "rw_threshold": RW,
+        "workload": f"{name}: {WORKLOADS[name]}, seed {SEED}, sc {SC}, rw {RW}",
+        "n": n, "m": m, "seed": SEED, "sc_threshold": SC, "rw_threshold": RW,
         "l2": "flushed before every step (256 MiB write)",
         "parallelism": "replicas",
     }
@@ -185,19 +208,32 @@ def product_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    g = G.grid3d(SIDE)
-    n, m = g.n, g.m
+    g, off_d, cols_d, n, m = load_workload(args.workload, dev)
     stream = torch.cuda.Stream(device=dev)
-    off_d = torch.from_numpy(g.offsets.view(np.int32)).to(dev)
-    cols_d = torch.from_numpy(g.cols.view(np.int32)).to(dev)
-    off_h = torch.from_numpy(g.offsets.view(np.int32)).pin_memory()
-    cols_h = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
+    if g is not None:
+        off_d = torch.from_numpy(g.offsets.view(np.int32)).to(dev)
+        cols_d = torch.from_numpy(g.cols.view(np.int32)).to(dev)
+        off_h = torch.from_numpy(g.offsets.view(np.int32)).pin_memory()
+        cols_h = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
+    else:
+        off_h = off_d.cpu().pin_memory()
+        cols_h = cols_d.cpu().pin_memory()
     off_hn = off_h.numpy().view(np.uint32)
     cols_hn = cols_h.numpy().view(np.uint32)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
-    dm = P.CudaDeviceManager(seed=SEED, sc_threshold=SC, rw_threshold=RW, device=local_rank,
-                             driver=P.DRIVER_GRAPH)
+    model = None
+    if args.schedule == "learned":
+        from parex_b200 import learn
+        model = learn.Model.load()
+
+    def manager(driver):
+        dmx = P.CudaDeviceManager(seed=SEED, sc_threshold=SC, rw_threshold=RW, device=local_rank, driver=driver)
+        if model is not None:
+            dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16)
+        return dmx
+
+    dm = manager(P.DRIVER_GRAPH)
     dm.set_stream(stream.cuda_stream)
 
     def barrier():
@@ -251,8 +287,7 @@ def product_arm(args, rank, world, local_rank):
         assert fp_e2e.numClusters == clusters
 
         # per-phase device times with the stream driver (roofline)
-        prof = P.CudaDeviceManager(seed=SEED, sc_threshold=SC, rw_threshold=RW, device=local_rank,
-                                   driver=P.DRIVER_STREAM)
+        prof = manager(P.DRIVER_STREAM)
         prof.set_stream(stream.cuda_stream)
         prof.initialize_device(n, m, off_d.data_ptr(), False, cols_d.data_ptr())
         prof.set_profiling(True)
@@ -305,16 +340,18 @@ def product_arm(args, rank, world, local_rank):
     }
 
     cpu = None
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and args.workload in ("grid128", "sbm16k"):
         res = run_reference_cpu(g, 1)
         cpu = {"value": m / res["secs"][0], "unit": UNIT, "cores": 1, "kind": res["kind"],
-               "sample": f"one full decomposition of the {SIDE}^3 grid ({res['secs'][0]:.1f} s, single thread)"}
+               "sample": f"one full decomposition of {args.workload} ({res['secs'][0]:.1f} s, single thread)"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(g, {"driver": "cuda graph, device-driven round loop", "rounds": rounds,
-                                      "clusters": clusters, "cut_edges_device": device_cut}),
+        "config": workload_config((n, m), {"driver": "cuda graph, device-driven round loop", "rounds": rounds,
+                                           "clusters": clusters, "cut_edges_device": device_cut,
+                                           "sweep_schedule": args.schedule, "row_plan": dm.row_plan()},
+                                  args.workload),
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms / args.steps},
@@ -333,6 +370,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="grid128", choices=sorted(WORKLOADS))
+    ap.add_argument("--schedule", default="plain", choices=["plain", "learned"])
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -315,6 +315,25 @@ pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* a
                          const double* x, const uint32_t* internal_degrees, const uint32_t* cols,
                          uint32_t n_clusters, int32_t smallest_label, int full_components);
 
+/* ---- graph construction on the device ------------------------------------
+ * The CSR the reference builds on the host (readDynGraph +
+ * DynamicGraph::finalize, lib/utils/graph_io.h:49-84, lib/core/graph.h:147-184),
+ * built on the GPU from an edge list in device memory: self-loops dropped,
+ * duplicate edges merged, both directions stored, rows sorted by neighbour.
+ * u, v: n_edges vertex ids (< n); offsets: n + 1 entries; cols: room for
+ * 2 * n_edges entries; scratch: pxr_build_csr_scratch_bytes(n_edges) bytes of
+ * device memory.  Needs 2 * n_edges < 2^32.  Synchronises the stream; *m_out
+ * is the number of undirected edges kept.  No counterpart in the reference's
+ * GPU code. */
+size_t pxr_build_csr_scratch_bytes(uint64_t n_edges);
+pxr_status pxr_build_csr(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
+                         uint32_t* offsets, uint32_t* cols, uint64_t* m_out, void* stream);
+/* R-MAT edge samples on the device: samples (u, v) pairs over 2^scale
+ * vertices, quadrant probabilities a, b, c (d = 1 - a - b - c), from the
+ * counter-based hash of parex_b200/graphs.py rmat() (same seed, same edges). */
+pxr_status pxr_rmat_edges(uint32_t scale, uint64_t samples, double a, double b, double c, uint64_t seed,
+                          uint32_t* u, uint32_t* v, void* stream);
+
 /* Learned sweep schedule: mode, trace and, for the learned modes, the MLP
  * (weights: PXR_MLP_PARAMS bf16 bit patterns, norm: 32 floats; host memory).
  * Takes effect from the next round; every cluster is due at (re)initialisation. */

@@ -31,7 +31,8 @@ SYMBOLS = [
     "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
     "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
-    "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan",
+    "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
+    "pxr_rmat_edges",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -162,6 +163,9 @@ def load() -> C.CDLL:
     L.pxr_initialize_batched.argtypes = [p, u32, u64, p, p, u32, p]
     L.pxr_set_schedule.argtypes = [p, C.POINTER(Schedule), p, p]
     L.pxr_get_row_plan.argtypes = [p, C.POINTER(RowPlan)]
+    L.pxr_build_csr_scratch_bytes.argtypes = [u64]
+    L.pxr_build_csr.argtypes = [u32, u64, p, p, p, p, p, C.POINTER(u64), p]
+    L.pxr_rmat_edges.argtypes = [u32, u64, C.c_double, C.c_double, C.c_double, u64, p, p, p]
     L.pxr_set_row_plan.argtypes = [p, C.POINTER(RowPlan)]
     L.pxr_read_cluster_records.argtypes = [p, p, u32, C.POINTER(u32)]
     L.pxr_mlp_forward.argtypes = [p, u32, p, p, p, p]
@@ -171,9 +175,10 @@ def load() -> C.CDLL:
     for name in SYMBOLS:
         fn = getattr(L, name)
         if name not in ("pxr_config_default", "pxr_status_string", "pxr_last_error", "pxr_destroy",
-                        "pxr_mlp_scratch_floats"):
+                        "pxr_mlp_scratch_floats", "pxr_build_csr_scratch_bytes"):
             fn.restype = C.c_int
     L.pxr_mlp_scratch_floats.restype = C.c_size_t
+    L.pxr_build_csr_scratch_bytes.restype = C.c_size_t
     _lib = L
     return L
 

@@ -1,0 +1,225 @@
+// Graph construction on the device (sm_100a): the reference builds its CSR
+// on the host (readDynGraph + DynamicGraph::finalize, lib/utils/graph_io.h:49-84,
+// lib/core/graph.h:147-184: self-loops dropped, both directions of every edge,
+// duplicates merged, rows sorted by neighbour id).  Here the same CSR comes from
+// two 64-bit radix sorts with this library's onesweep sort:
+//
+//   1. pack every non-loop edge as (min << 32 | max) (compaction by atomic
+//      counter: the order is irrelevant, a sort follows);
+//   2. sort, keep the first of each run of equal keys, emit both directions
+//      (src << 32 | dst);
+//   3. sort again: the low words are the columns, row starts come from a
+//      binary search for each vertex.
+//
+// Also an R-MAT edge sampler with the counter-based hash of the Python
+// generator (parex_b200/graphs.py: rmat), so both produce the same graph.
+#include <algorithm>
+#include <cmath>
+
+#include "pxr_sort.cuh"
+#include "../../include/parex_b200.h"
+
+namespace pxr {
+namespace {
+
+constexpr int kBuildBlock = 256;
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// One quadrant choice per bit level from a 16-bit uniform; four levels per
+// 64-bit hash of (seed, stream 1000 + level / 4, sample index).
+__global__ void k_rmat(uint64_t samples, uint32_t scale, uint32_t ta, uint32_t tab, uint32_t tabc, uint64_t seed,
+                       uint32_t* u, uint32_t* v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < samples;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t uu = 0, vv = 0;
+        uint64_t h = 0;
+        for (uint32_t lvl = 0; lvl < scale; ++lvl) {
+            if ((lvl & 3u) == 0) {
+                const uint64_t base = seed * 0x100000001B3ull + (uint64_t)(1000u + lvl / 4u) * 0x9E3779B1ull;
+                h = splitmix64(splitmix64(i ^ base) + base);
+            }
+            const uint32_t r = (uint32_t)(h >> (16u * (lvl & 3u))) & 0xFFFFu;
+            const uint32_t bit = 1u << (scale - 1u - lvl);
+            if (r >= tab) uu |= bit;
+            if ((r >= ta && r < tab) || r >= tabc) vv |= bit;
+        }
+        u[i] = uu;
+        v[i] = vv;
+    }
+}
+
+__global__ void k_pack_edges(const uint32_t* u, const uint32_t* v, uint64_t n_edges, uint32_t n, uint64_t* keys,
+                             uint32_t* count, uint32_t* bad) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_edges;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = u[i], b = v[i];
+        if (a >= n || b >= n) { atomicOr(bad, 1u); continue; }
+        if (a == b) continue;
+        const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+        keys[atomicAdd(count, 1u)] = ((uint64_t)lo << 32) | hi;
+    }
+}
+
+// first of each run of equal sorted keys -> both directions
+__global__ void k_unique_both(const uint64_t* sorted0, const uint64_t* sorted1, const uint32_t* sel,
+                              const uint32_t* count, uint64_t* out, uint32_t* out_count) {
+    const uint64_t* k = *sel ? sorted1 : sorted0;
+    const uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t key = k[i];
+        if (i > 0 && k[i - 1] == key) continue;
+        const uint32_t lo = (uint32_t)(key >> 32), hi = (uint32_t)key;
+        const uint32_t p = atomicAdd(out_count, 2u);
+        out[p] = key;
+        out[p + 1] = ((uint64_t)hi << 32) | lo;
+    }
+}
+
+// columns and row starts of the sorted (src, dst) list
+__global__ void k_csr_rows(const uint64_t* sorted0, const uint64_t* sorted1, const uint32_t* sel, const uint32_t* count,
+                           uint32_t n, uint32_t* offsets, uint32_t* cols) {
+    const uint64_t* k = *sel ? sorted1 : sorted0;
+    const uint32_t total = *count;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = tid; i < total; i += stride) cols[i] = (uint32_t)k[i];
+    for (uint64_t v = tid; v <= n; v += stride) {
+        const uint64_t target = v << 32;
+        uint32_t lo = 0, hi = total;   // first position with key >= target
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (k[mid] < target) lo = mid + 1; else hi = mid;
+        }
+        offsets[v] = lo;
+    }
+}
+
+__global__ void k_set_u32(uint32_t* p, uint32_t value) { *p = value; }
+
+struct BuildLayout {
+    size_t keys0, keys1, hist, bases, pass_info, tile_ctr, epoch, status, words, total;
+    uint32_t tiles;
+};
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+BuildLayout build_layout(uint64_t n_edges) {
+    BuildLayout L{};
+    const uint64_t cap = std::max<uint64_t>(2 * n_edges, 1);
+    L.tiles = (uint32_t)((cap + kSortTile - 1) / kSortTile) + 1;
+    size_t o = 0;
+    L.keys0 = o; o = align256(o + cap * 8);
+    L.keys1 = o; o = align256(o + cap * 8);
+    L.hist = o; o = align256(o + kMaxPasses * kRadix * 4);
+    L.bases = o; o = align256(o + kMaxPasses * kRadix * 4);
+    L.pass_info = o; o = align256(o + (kMaxPasses + 1) * 4);
+    L.tile_ctr = o; o = align256(o + kMaxPasses * 4);
+    L.epoch = o; o = align256(o + 4);
+    L.status = o; o = align256(o + (size_t)L.tiles * kRadix * 8);
+    L.words = o; o = align256(o + 8 * 4);   // count0, count1, end_bit, err, bad
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+}  // namespace pxr
+
+using namespace pxr;
+
+extern "C" {
+
+pxr_status pxr_rmat_edges(uint32_t scale, uint64_t samples, double a, double b, double c, uint64_t seed, uint32_t* u,
+                          uint32_t* v, void* stream) {
+    if (scale == 0 || scale > 31 || (samples && (!u || !v))) return PXR_INVALID_ARG;
+    if (!(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0)) return PXR_INVALID_ARG;
+    if (!samples) return PXR_OK;
+    // quadrant thresholds on a 16-bit uniform, rounded half to even as the Python generator does
+    const uint32_t ta = (uint32_t)std::nearbyint(a * 65536.0);
+    const uint32_t tab = (uint32_t)std::nearbyint((a + b) * 65536.0);
+    const uint32_t tabc = (uint32_t)std::nearbyint((a + b + c) * 65536.0);
+    const uint64_t blocks = std::min<uint64_t>((samples + kBuildBlock - 1) / kBuildBlock, 148u * 32u);
+    k_rmat<<<(uint32_t)blocks, kBuildBlock, 0, static_cast<cudaStream_t>(stream)>>>(samples, scale, ta, tab, tabc,
+                                                                                    seed, u, v);
+    return cudaGetLastError() == cudaSuccess ? PXR_OK : PXR_CUDA_ERROR;
+}
+
+size_t pxr_build_csr_scratch_bytes(uint64_t n_edges) { return build_layout(n_edges).total; }
+
+pxr_status pxr_build_csr(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
+                         uint32_t* offsets, uint32_t* cols, uint64_t* m_out, void* stream) {
+    if (!offsets || !m_out || (n_edges && (!u || !v || !cols || !scratch))) return PXR_INVALID_ARG;
+    if (n >= 0x7FFFFFFFu || 2 * n_edges >= (1ull << 32)) return PXR_INVALID_ARG;   // 32-bit item counts and offsets
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    static bool prepared[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (dev >= 0 && dev < 64 && !prepared[dev]) {
+        if (radix_sort_prepare<uint64_t>() != cudaSuccess) return PXR_CUDA_ERROR;
+        prepared[dev] = true;
+    }
+    const BuildLayout L = build_layout(n_edges);
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    uint64_t* k0 = reinterpret_cast<uint64_t*>(base + L.keys0);
+    uint64_t* k1 = reinterpret_cast<uint64_t*>(base + L.keys1);
+    uint32_t* words = reinterpret_cast<uint32_t*>(base + L.words);
+    uint32_t *count0 = words, *count1 = words + 1, *end_bit = words + 2, *err = words + 3, *bad = words + 4;
+    // sort state starts zeroed (histograms, epochs, status words)
+    if (cudaMemsetAsync(base + L.hist, 0, L.total - L.hist, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    uint32_t bits = 0;
+    while (bits < 32 && (1ull << bits) < n) ++bits;
+    k_set_u32<<<1, 1, 0, s>>>(end_bit, 32u + bits);
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((std::max<uint64_t>(n_edges, (uint64_t)n + 1) + kBuildBlock - 1) /
+                                                           kBuildBlock, 148u * 32u);
+    if (n_edges) k_pack_edges<<<grid, kBuildBlock, 0, s>>>(u, v, n_edges, n, k0, count0, bad);
+    SortState st{};
+    st.hist = reinterpret_cast<uint32_t*>(base + L.hist);
+    st.bases = reinterpret_cast<uint32_t*>(base + L.bases);
+    st.pass_info = reinterpret_cast<uint32_t*>(base + L.pass_info);
+    st.tile_ctr = reinterpret_cast<uint32_t*>(base + L.tile_ctr);
+    st.epoch = reinterpret_cast<uint32_t*>(base + L.epoch);
+    st.status = reinterpret_cast<uint64_t*>(base + L.status);
+    st.max_tiles = L.tiles;
+    st.items_moved = nullptr;
+    SortBuffers<uint64_t> b{};
+    b.keys[0] = k0;
+    b.keys[1] = k1;
+    b.count = count0;
+    b.end_bit = end_bit;
+    b.capacity = (uint32_t)n_edges;
+    if (radix_sort<uint64_t>(b, st, err, s, 64) != cudaSuccess) return PXR_CUDA_ERROR;
+    // the unique pass writes into the buffer the sort did not end in
+    const uint32_t* sel = st.pass_info + kMaxPasses;
+    uint32_t sel_host = 0;
+    if (cudaMemcpyAsync(&sel_host, sel, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    uint64_t* uniq = sel_host ? k0 : k1;
+    if (n_edges) k_unique_both<<<grid, kBuildBlock, 0, s>>>(k0, k1, sel, count0, uniq, count1);
+    SortBuffers<uint64_t> b2{};
+    b2.keys[0] = uniq;
+    b2.keys[1] = sel_host ? k1 : k0;
+    b2.count = count1;
+    b2.end_bit = end_bit;
+    b2.capacity = (uint32_t)(2 * n_edges);
+    if (radix_sort<uint64_t>(b2, st, err, s, 64) != cudaSuccess) return PXR_CUDA_ERROR;
+    // result buffer of the second sort relative to b2: pass_info[kMaxPasses] selects keys[0] or keys[1]
+    uint32_t sel2 = 0;
+    if (cudaMemcpyAsync(&sel2, sel, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    k_csr_rows<<<grid, kBuildBlock, 0, s>>>(b2.keys[0], b2.keys[1], sel, count1, n, offsets, cols);
+    uint32_t w[5] = {0, 0, 0, 0, 0};
+    if (cudaMemcpyAsync(w, words, 20, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    (void)sel2;
+    if (w[4]) return PXR_INVALID_ARG;   // a vertex id >= n
+    if (w[3]) return PXR_DEVICE_FAULT;  // a sort wait ran out
+    *m_out = w[1] / 2;
+    return PXR_OK;
+}
+
+}  // extern "C"

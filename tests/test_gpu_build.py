@@ -1,0 +1,70 @@
+"""Device CSR construction (pxr_build_csr) and the device R-MAT sampler
+(pxr_rmat_edges) against the host builders in parex_b200/graphs.py: the
+same CSR, slot for slot."""
+import numpy as np
+import pytest
+import torch
+
+import parex_b200 as P
+from parex_b200 import graphs as G
+from parex_b200 import gpu_build as B
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).cuda()
+
+
+def _same(g_dev, g_host):
+    np.testing.assert_array_equal(g_dev.offsets.astype(np.int64), g_host.offsets.astype(np.int64))
+    np.testing.assert_array_equal(g_dev.cols, g_host.cols)
+
+
+@pytest.mark.parametrize("scale,abc,seed", [(10, (0.57, 0.19, 0.19), 1), (12, (0.57, 0.19, 0.19), 3),
+                                            (11, (0.45, 0.15, 0.15), 7)])
+def test_rmat_matches_host_generator(scale, abc, seed):
+    off, cols, n, m = B.rmat(scale, 16, *abc, seed=seed)
+    host = G.rmat(scale, 16, *abc, seed=seed)
+    assert n == host.n and m == host.m
+    _same(B.to_host(off, cols), host)
+
+
+def test_multigraph_with_loops_and_duplicates():
+    rng = np.random.default_rng(5)
+    n = 5000
+    u = rng.integers(0, n, 60000)
+    v = rng.integers(0, n, 60000)
+    u = np.concatenate([u, v[:1000], np.arange(100)])         # reversed duplicates and self-loops
+    v = np.concatenate([v, u[:1000], np.arange(100)])
+    off, cols, m = B.build_csr(n, _dev(u), _dev(v))
+    host = G.csr_from_edges(u, v, n)
+    assert m == host.m
+    _same(B.to_host(off, cols), host)
+
+
+def test_grid_and_empty_cases():
+    host = G.grid3d(10)
+    src = np.repeat(np.arange(host.n), np.diff(host.offsets.astype(np.int64)))
+    off, cols, m = B.build_csr(host.n, _dev(src), _dev(host.cols))   # every edge twice, both ways
+    _same(B.to_host(off, cols), host)
+    off, cols, m = B.build_csr(7, _dev(np.zeros(0)), _dev(np.zeros(0)))
+    assert m == 0 and np.all(off.cpu().numpy() == 0)
+    off, cols, m = B.build_csr(3, _dev([0, 1, 2]), _dev([0, 1, 2]))  # only self-loops
+    assert m == 0
+
+
+def test_out_of_range_vertex_is_refused():
+    with pytest.raises(P.PxrError):
+        B.build_csr(10, _dev([1, 2, 11]), _dev([2, 3, 4]))
+
+
+def test_device_csr_decomposes_like_host_csr():
+    off, cols, n, m = B.rmat(13, 16, seed=2)
+    a = P.CudaDeviceManager()
+    a.initialize_device(n, m, off.data_ptr(), False, cols.data_ptr())
+    a.expanderDecomposition()
+    b = P.CudaDeviceManager()
+    b.initialize(G.rmat(13, 16, seed=2))
+    b.expanderDecomposition()
+    np.testing.assert_array_equal(a.getFinalPartition().clusterIds, b.getFinalPartition().clusterIds)
