@@ -229,6 +229,8 @@ def product_arm(args, rank, world, local_rank):
 
     def manager(driver):
         dmx = P.CudaDeviceManager(seed=SEED, sc_threshold=SC, rw_threshold=RW, device=local_rank, driver=driver)
+        if args.row_plan:
+            dmx.set_row_plan(*[int(t) for t in args.row_plan.split(",")])
         if model is not None:
             dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16)
         return dmx
@@ -372,6 +374,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="grid128", choices=sorted(WORKLOADS))
     ap.add_argument("--schedule", default="plain", choices=["plain", "learned"])
+    ap.add_argument("--row-plan", default=None, help="force lanes_per_row,light_max,wide_max (default: autotuned)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -48,7 +48,12 @@ struct RoundCtr {
     uint32_t loop_cap;        // round cap of the device-driven loop
     uint32_t n_sweep;         // vertices in this round's sweep (all active ones in the plain form)
     uint32_t n_due_items;     // vertices of the clusters swept and acted on this round
-    uint32_t pad0;
+    uint32_t chunk_path;      // this round's sort runs chunk by chunk in shared memory
+    uint32_t n_gsort;         // items of the global sort (0 on the chunk path)
+    uint32_t max_parent;      // largest cluster of the previous round (bounds the active list's runs)
+    uint32_t max_csize;       // largest cluster of this round
+    uint32_t max_csize_next;  // largest cluster kept for the next round
+    uint32_t pad0, pad1;
     unsigned long long stat_walk_vertices;  // traffic counters since initialisation
     unsigned long long stat_walk_slots;
     unsigned long long stat_walk_gathers;

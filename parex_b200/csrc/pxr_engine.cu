@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "pxr_sched.cuh"
+#include "pxr_chunk.cuh"
 
 using namespace pxr;
 
@@ -259,6 +260,7 @@ struct pxr_handle {
     uint32_t* pvol = nullptr;
     uint32_t* act[2] = {nullptr, nullptr};
     uint32_t* ids[2] = {nullptr, nullptr};
+    uint32_t* par[2] = {nullptr, nullptr};   // per active-list position: cluster it was last swept in
     uint64_t* keys[2] = {nullptr, nullptr};
     uint32_t* vals[2] = {nullptr, nullptr};
     ClusterTables tab[2]{};
@@ -517,11 +519,17 @@ cudaError_t op_sweep(pxr_handle* h) {
     SortBuffers<uint64_t> b{};
     b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
     b.vals[0] = h->vals[0]; b.vals[1] = h->vals[1];
-    b.count = &h->ctr->n_sweep;
+    // the learned schedule sets the sweep size after the round's preparation
+    b.count = h->sched.mode ? &h->ctr->n_sweep : &h->ctr->n_gsort;
     b.end_bit = h->sort_end_bit;
     b.capacity = h->n;
     cudaError_t e = cudaSuccess;
-    phase(h, kPhSort, 2 + kMaxPasses, [&] { e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64); });
+    phase(h, kPhSort, 3 + kMaxPasses, [&] {
+        e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64);
+        // the chunked sort writes buffer 0, which the idle global sort leaves selected
+        k_chunk_sort<OffT><<<std::min(std::max((h->n + kChunk - 1) / kChunk, 1u), 148u), kChunkThreads, chunk_sort_smem(), s>>>(
+            d, t, h->act[h->acur], h->par[h->acur], h->keys[0], h->vals[0]);
+    });
     if (e != cudaSuccess) return e;
     phase(h, kPhScan, 1, [&] {
         k_sweep_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->keys[0], h->keys[1], h->vals[0], h->vals[1]);
@@ -576,7 +584,7 @@ cudaError_t op_cut(pxr_handle* h) {
         });
     phase(h, kPhApply, 1, [&] {
         k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
-                                               h->act[h->acur ^ 1]);
+                                               h->act[h->acur ^ 1], h->par[h->acur ^ 1]);
     });
     phase(h, kPhDisable, 1 + long_launches(h), [&] {
         k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
@@ -778,7 +786,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->dv, N); A(&h->parent, N); A(&h->acc_max, N); A(&h->acc_min, N); A(&h->acc_cnt, N);
     A(&h->acc_sum, N); A(&h->newlab, N); A(&h->avg, N); A(&h->pdif, N); A(&h->pvol, N);
     for (int i = 0; i < 2; ++i) {
-        A(&h->act[i], N); A(&h->ids[i], N); A(&h->keys[i], N); A(&h->vals[i], N); A(&h->roots[i], N);
+        A(&h->act[i], N); A(&h->ids[i], N); A(&h->par[i], N); A(&h->keys[i], N); A(&h->vals[i], N); A(&h->roots[i], N);
         A(&h->tab[i].start, N); A(&h->tab[i].size, N); A(&h->tab[i].vol, N); A(&h->tab[i].vol_start, N);
         A(&h->tab[i].root, N); A(&h->tab[i].best, N); A(&h->tab[i].skip, N); A(&h->tab[i].hist, N);
     }
@@ -1046,6 +1054,8 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     c.full_components = 1;
     c.done = n ? 0u : 1u;
     c.main_sel = old.main_sel;
+    c.max_parent = 0xFFFFFFFFu;   // the first round sorts globally (the list is in vertex order)
+    c.max_csize = n;
     PXR_CUDA(h, cudaMemcpyAsync(h->ctr, &c, sizeof(RoundCtr), cudaMemcpyHostToDevice, s));
     if (n) {
         k_degrees<OffT><<<grid_for(n), kBlock, 0, s>>>(static_cast<const OffT*>(h->off), n, h->ideg, h->lab,
@@ -1174,11 +1184,13 @@ pxr_status pxr_create(const pxr_config* cfg, pxr_handle** out) {
     }
     std::memset(h->h_ctr, 0, sizeof(RoundCtr));
     h->stream = h->own_stream;
-    static bool attrs_set = false;
-    if (!attrs_set) {
+    static bool attrs_set[64] = {};   // function attributes are per device
+    if (h->device < 64 && !attrs_set[h->device]) {
         radix_sort_prepare<uint64_t>();
         radix_sort_prepare<uint32_t>();
-        attrs_set = true;
+        cudaFuncSetAttribute(k_chunk_sort<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chunk_sort_smem());
+        cudaFuncSetAttribute(k_chunk_sort<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chunk_sort_smem());
+        attrs_set[h->device] = true;
     }
     *out = h;
     return PXR_OK;
@@ -1546,6 +1558,8 @@ pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* a
     c->smallest = smallest;
     c->full_components = full_components ? 1u : 0u;
     c->done = (n_act == 0 || n_clusters == 0) ? 1u : 0u;
+    c->max_parent = 0xFFFFFFFFu;   // the given list has no run structure: sort globally first
+    c->max_csize = n;
     PXR_CUDA(h, cudaMemcpyAsync(h->ctr, c, sizeof(RoundCtr), cudaMemcpyHostToDevice, s));
     pxr_status rs = reset_schedule_state(h);
     if (rs != PXR_OK) return rs;

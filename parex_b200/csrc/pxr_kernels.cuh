@@ -154,6 +154,12 @@ __global__ void k_round_prep(Dev<OffT> d, int stage) {
         if (d.sched) c->n_sweep = 0;   // set by k_due_scan
     }
     if (!d.sched) c->n_sweep = c->n_active;
+    if (stage == 1) {
+        // every previous cluster fits a chunk: sort in shared memory (pxr_chunk.cuh)
+        c->chunk_path = (!d.sched && c->max_parent <= kChunkCapRows && c->n_active > 0) ? 1u : 0u;
+        c->n_gsort = c->chunk_path ? 0u : c->n_sweep;
+    }
+    if (stage == 2) c->max_csize_next = 0;
     const uint32_t k = c->n_clusters;
     *d.sort_end_bit = 32u + bitlen(k > 0 ? k - 1 : 0);
 }
@@ -168,6 +174,10 @@ __global__ void k_round_end(Dev<OffT> d) {
         c->rounds += 1;
         c->stat_swept_items += c->n_sweep;
     }
+    // the next active list holds this round's clusters as contiguous runs
+    // (the learned schedule appends carried clusters: no chunk path)
+    c->max_parent = d.sched ? 0xFFFFFFFFu : c->max_csize;
+    c->max_csize = c->max_csize_next;
     c->n_active = c->n_active_next;
     c->n_clusters = c->n_keep;
     c->smallest = c->smallest_next;
@@ -207,14 +217,17 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
         const bool light = valid && (uint64_t)(end - beg) <= d.light_max;
         if (!light) beg = end;      // long rows: k_walk_long
         int64_t acc = 0;
-        for (OffT s = beg + gl; s < end; s += 4 * W) {
-            uint32_t nb[4];
+        for (OffT s = beg + gl; s < end; s += kSlotUnroll * W) {
+            uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            float xv[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kSlotUnroll; ++u) xv[u] = nb[u] != kInvalidEdge ? xt_in[nb[u]] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < kSlotUnroll; ++u) {
                 st_s += s + u * W < end ? 1 : 0;
-                if (nb[u] != kInvalidEdge) { acc += to_fixed(xt_in[nb[u]], scale); ++st_g; }
+                if (nb[u] != kInvalidEdge) { acc += to_fixed(xv[u], scale); ++st_g; }
             }
         }
         st_v += (light && gl == 0) ? 1 : 0;
@@ -269,14 +282,17 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
         const bool light = in && (uint64_t)(end - beg) <= d.light_max;
         if (!light) beg = end;      // long rows: k_nodediff_long
         int32_t c = 0;
-        for (OffT s = beg + gl; s < end; s += 4 * W) {
-            uint32_t nb[4];
+        for (OffT s = beg + gl; s < end; s += kSlotUnroll * W) {
+            uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            float xn[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kSlotUnroll; ++u) xn[u] = nb[u] != kInvalidEdge ? d.x[nb[u]] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < kSlotUnroll; ++u) {
                 if (nb[u] == kInvalidEdge) continue;
-                const uint32_t o = ordered_bits(d.x[nb[u]]);
+                const uint32_t o = ordered_bits(xn[u]);
                 const bool before = o < mine || (o == mine && nb[u] < v);
                 c += before ? -1 : 1;
             }
@@ -293,10 +309,13 @@ __global__ void __launch_bounds__(kBlock) k_emit(Dev<OffT> d, const uint32_t* ac
                                                  uint32_t* vals, uint64_t* best) {
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
+    const bool emit = !d.ctr->chunk_path;   // the chunk path reads the active list itself
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const uint32_t v = act[i];
-        keys[i] = ((uint64_t)(uint32_t)d.lab[v] << 32) | ordered_bits(d.x[v]);
-        vals[i] = v;
+        if (emit) {
+            const uint32_t v = act[i];
+            keys[i] = ((uint64_t)(uint32_t)d.lab[v] << 32) | ordered_bits(d.x[v]);
+            vals[i] = v;
+        }
         if (i < k) best[i] = ~0ull;
     }
 }
@@ -671,6 +690,7 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
     const uint32_t hi = (uint32_t)(incl >> 32) - (uint32_t)(run >> 32);
     uint64_t p = PairAdd::combine(s_excl, ((uint64_t)hi << 32) | lo);
     int32_t most_negative = 0;
+    uint32_t biggest = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const uint32_t j = first + k;
@@ -679,6 +699,7 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
         if (vals[k]) {
             const uint32_t nl = (uint32_t)p;
             const uint32_t cnt = (uint32_t)(vals[k] >> 32);
+            biggest = cnt > biggest ? cnt : biggest;
             d.newlab[r] = (int32_t)nl;
             d.avg[r] = __ddiv_rn(__dmul_rn(__ll2double_rn(d.acc_sum[r]), inv), (double)cnt);
             nt.size[nl] = cnt;
@@ -707,6 +728,9 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) most_negative = min(most_negative, __shfl_xor_sync(0xFFFFFFFFu, most_negative, o));
     if ((threadIdx.x & 31u) == 0 && most_negative < 0) atomicMin(&d.ctr->smallest_next, most_negative);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) biggest = max(biggest, __shfl_xor_sync(0xFFFFFFFFu, biggest, o));
+    if ((threadIdx.x & 31u) == 0 && biggest) atomicMax(&d.ctr->max_csize_next, biggest);
 }
 
 // new labels, recentering (x -= cluster mean) and the stable compaction of
@@ -714,7 +738,7 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                   const uint32_t* vals1, const uint64_t* keys0,
-                                                  const uint64_t* keys1, uint32_t* act_next) {
+                                                  const uint64_t* keys1, uint32_t* act_next, uint32_t* par_next) {
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_sweep;
@@ -727,14 +751,16 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
     const uint64_t* keys = sel ? keys1 : keys0;
     const uint32_t epoch = d.lb_epoch[kSiteApply];
     const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
-    uint32_t vv[kScanItems];
+    uint32_t vv[kScanItems], cc[kScanItems];
     uint32_t keepmask = 0, run = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const uint32_t i = first + k;
         vv[k] = 0;
+        cc[k] = 0;
         if (i >= count) continue;
         const uint32_t c = (uint32_t)(keys[i] >> 32);
+        cc[k] = c;
         if (d.sched && !(d.sflag[c] & 1u)) continue;   // carried: k_carry_vertices
         const uint32_t v = vals[i];
         vv[k] = v;
@@ -759,7 +785,11 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
     uint32_t pos = (uint32_t)(s_excl + incl - run);
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k)
-        if (keepmask & (1u << k)) act_next[pos++] = vv[k];
+        if (keepmask & (1u << k)) {
+            act_next[pos] = vv[k];
+            par_next[pos] = cc[k];   // the cluster the vertex was swept in: runs of the next list
+            ++pos;
+        }
 }
 
 // next round's vertex-order list, edge disabling (disableEdgesKernel_node,
@@ -828,15 +858,15 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         const bool light = valid && (uint64_t)(end - beg) <= d.light_max;
         if (!light || noscan) beg = end;      // long rows: k_disable_long
         uint32_t deg = 0;
-        for (OffT s = beg + gl; s < end; s += 4 * W) {
-            uint32_t nb[4];
+        for (OffT s = beg + gl; s < end; s += kSlotUnroll * W) {
+            uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
-            int32_t ln[4];
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            int32_t ln[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) ln[u] = nb[u] != kInvalidEdge ? d.lab[nb[u]] : lv;
+            for (int u = 0; u < kSlotUnroll; ++u) ln[u] = nb[u] != kInvalidEdge ? d.lab[nb[u]] : lv;
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kSlotUnroll; ++u) {
                 if (nb[u] == kInvalidEdge) continue;
                 if (ln[u] != lv) d.cols[s + u * W] = kInvalidEdge;
                 else ++deg;
@@ -879,7 +909,7 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
 // Long rows.  Rows longer than Dev::light_max slots are binned once per graph
 // into two static lists: "wide" rows (up to Dev::wide_max slots) get one warp
 // each, "heavy" rows one CTA each (G = 32 or kBlock lanes per row, slots
-// strided by G with four independent loads per step, group reduction).
+// strided by G with kSlotUnroll independent loads per step, group reduction).
 // Every accumulation is order-independent, so the binning does not change
 // any result.
 
@@ -948,13 +978,16 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
         const OffT beg = d.off[v], end = d.off[v + 1];
         int64_t acc = 0;
         unsigned long long g = 0;
-        for (OffT s = beg + rg.lane; s < end; s += 4 * G) {
-            uint32_t nb[4];
+        for (OffT s = beg + rg.lane; s < end; s += kSlotUnroll * G) {
+            uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
+            float xv[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (nb[u] != kInvalidEdge) { acc += to_fixed(xt_in[nb[u]], scale); ++g; }
+            for (int u = 0; u < kSlotUnroll; ++u) xv[u] = nb[u] != kInvalidEdge ? xt_in[nb[u]] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < kSlotUnroll; ++u)
+                if (nb[u] != kInvalidEdge) { acc += to_fixed(xv[u], scale); ++g; }
         }
         acc = group_sum<G, int64_t>(acc, sh);
         st_g += g;
@@ -1002,14 +1035,17 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
         const uint32_t mine = ordered_bits(d.x[v]);
         const OffT beg = d.off[v], end = d.off[v + 1];
         int32_t c = 0;
-        for (OffT s = beg + rg.lane; s < end; s += 4 * G) {
-            uint32_t nb[4];
+        for (OffT s = beg + rg.lane; s < end; s += kSlotUnroll * G) {
+            uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
+            float xn[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kSlotUnroll; ++u) xn[u] = nb[u] != kInvalidEdge ? d.x[nb[u]] : 0.0f;
+#pragma unroll
+            for (int u = 0; u < kSlotUnroll; ++u) {
                 if (nb[u] == kInvalidEdge) continue;
-                const uint32_t o = ordered_bits(d.x[nb[u]]);
+                const uint32_t o = ordered_bits(xn[u]);
                 c += (o < mine || (o == mine && nb[u] < v)) ? -1 : 1;
             }
         }

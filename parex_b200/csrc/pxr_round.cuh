@@ -116,7 +116,16 @@ struct Dev {
 // Default row bins: rows up to kLightRow slots go W lanes per row, up to
 // kWideRow a warp per row, longer rows a CTA per row.
 constexpr uint32_t kLightRow = 64;
+// Slots a lane loads before it gathers their neighbours' values (loads in
+// flight per lane in the row kernels).
+#ifndef PXR_SLOT_UNROLL
+#define PXR_SLOT_UNROLL 4
+#endif
+constexpr int kSlotUnroll = PXR_SLOT_UNROLL;
 constexpr uint32_t kWideRow = 4096;
+// Largest previous-round cluster for which a round's sort runs chunk by
+// chunk in shared memory (pxr_chunk.cuh).
+constexpr uint32_t kChunkCapRows = 4096;
 
 // look-back sites (index into Dev::lb_epoch and RoundCtr::tile_counter)
 enum : int {
