@@ -53,7 +53,8 @@ struct RoundCtr {
     uint32_t max_parent;      // largest cluster of the previous round (bounds the active list's runs)
     uint32_t max_csize;       // largest cluster of this round
     uint32_t max_csize_next;  // largest cluster kept for the next round
-    uint32_t pad0, pad1;
+    uint32_t walk_only;       // learned schedule: no cluster is due this round, only the walk runs
+    uint32_t pad1;
     unsigned long long stat_walk_vertices;  // traffic counters since initialisation
     unsigned long long stat_walk_slots;
     unsigned long long stat_walk_gathers;

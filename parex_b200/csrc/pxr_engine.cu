@@ -505,7 +505,10 @@ cudaError_t op_sweep(pxr_handle* h) {
     phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1); });
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     if (h->sched.mode)
-        phase(h, kPhSched, 1, [&] { k_due_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t); });
+        phase(h, kPhSched, 2, [&] {
+            k_due_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t);
+            k_walk_only_check<OffT><<<1, 1, 0, s>>>(d);
+        });
     phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
         k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
         PXR_LONG(h, k_nodediff_long, d);
@@ -549,7 +552,11 @@ cudaError_t op_cut(pxr_handle* h) {
     hold_for_profiling(h);
     phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 2); });
     if (h->sched.mode)
-        phase(h, kPhSched, 1, [&] { k_carry_roots<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->roots[0]); });
+        phase(h, kPhSched, 2, [&] {
+            k_carry_all<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, nt, h->act[h->acur], h->act[h->acur ^ 1],
+                                                                 h->ids[h->acur], h->ids[h->acur ^ 1]);
+            k_carry_roots<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->roots[0]);
+        });
     phase(h, kPhCutInit, 1, [&] {
         k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });

@@ -132,6 +132,10 @@ __device__ __forceinline__ uint32_t fetch_tile(RoundCtr* ctr, int site) {
 __device__ __forceinline__ uint32_t sorted_sel(const SortState& s) { return s.pass_info[kMaxPasses]; }
 
 
+// Column indices are read once per round and stream through: load them with
+// an evict-first hint so that the potentials the gathers read stay in L2.
+__device__ __forceinline__ uint32_t stream_col(const uint32_t* p) { return __ldcs(p); }
+
 // ---------------------------------------------------------------------------
 // round bookkeeping
 
@@ -141,7 +145,10 @@ __global__ void k_round_prep(Dev<OffT> d, int stage) {
     RoundCtr* c = d.ctr;
     c->n_cut = 0;
     c->n_roots = 0;
-    if (stage == 0) c->xmax_walk_bits = 0;
+    if (stage == 0) {
+        c->xmax_walk_bits = 0;
+        c->walk_only = 0;
+    }
     c->smallest_next = 0;
     c->n_keep = 0;
     c->n_active_next = 0;
@@ -220,7 +227,7 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
         for (OffT s = beg + gl; s < end; s += kSlotUnroll * W) {
             uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? stream_col(d.cols + s + u * W) : kInvalidEdge;
             float xv[kSlotUnroll];
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) xv[u] = nb[u] != kInvalidEdge ? xt_in[nb[u]] : 0.0f;
@@ -267,6 +274,7 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
 
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t* ids) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t count = d.ctr->n_active;
     const uint32_t gl = threadIdx.x & (W - 1);
     const uint32_t groups = (gridDim.x * blockDim.x) / W;
@@ -285,7 +293,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
         for (OffT s = beg + gl; s < end; s += kSlotUnroll * W) {
             uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? stream_col(d.cols + s + u * W) : kInvalidEdge;
             float xn[kSlotUnroll];
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) xn[u] = nb[u] != kInvalidEdge ? d.x[nb[u]] : 0.0f;
@@ -416,6 +424,7 @@ __global__ void __launch_bounds__(kBlock) k_sweep_scan(Dev<OffT> d, ClusterTable
 // cuda/devSweepCut.h:321-331, 701-709) and the components plan.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTables t) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t full = d.ctr->full_components;
     pxr_sweep_cut* cuts = reinterpret_cast<pxr_sweep_cut*>(d.allcuts);
@@ -739,6 +748,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                   const uint32_t* vals1, const uint64_t* keys0,
                                                   const uint64_t* keys1, uint32_t* act_next, uint32_t* par_next) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_sweep;
@@ -797,6 +807,7 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint32_t* ids, uint32_t* ids_next,
                                                         float* xt, ClusterTables nt) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     __shared__ uint32_t s_list[kScanTile];
@@ -861,7 +872,7 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
         for (OffT s = beg + gl; s < end; s += kSlotUnroll * W) {
             uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? d.cols[s + u * W] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? stream_col(d.cols + s + u * W) : kInvalidEdge;
             int32_t ln[kSlotUnroll];
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) ln[u] = nb[u] != kInvalidEdge ? d.lab[nb[u]] : lv;
@@ -981,7 +992,7 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
         for (OffT s = beg + rg.lane; s < end; s += kSlotUnroll * G) {
             uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? stream_col(d.cols + s + u * G) : kInvalidEdge;
             float xv[kSlotUnroll];
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) xv[u] = nb[u] != kInvalidEdge ? xt_in[nb[u]] : 0.0f;
@@ -1023,6 +1034,7 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ int32_t sh[kBlock / 32];
     uint32_t cnt;
     const uint32_t* list = row_list(d, G, &cnt);
@@ -1038,7 +1050,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
         for (OffT s = beg + rg.lane; s < end; s += kSlotUnroll * G) {
             uint32_t nb[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? d.cols[s + u * G] : kInvalidEdge;
+            for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? stream_col(d.cols + s + u * G) : kInvalidEdge;
             float xn[kSlotUnroll];
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) xn[u] = nb[u] != kInvalidEdge ? d.x[nb[u]] : 0.0f;
@@ -1056,6 +1068,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     uint32_t cnt;
     const uint32_t* list = row_list(d, G, &cnt);
@@ -1086,6 +1099,7 @@ __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt, ClusterTables nt) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint32_t sh[kBlock / 32];
     uint32_t cnt;
     const uint32_t* list = row_list(d, G, &cnt);
@@ -1122,6 +1136,7 @@ __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt,
 // exclusive prefix of cluster volumes over labels
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cvol_scan(Dev<OffT> d, ClusterTables nt) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_keep;

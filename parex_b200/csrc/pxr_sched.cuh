@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(kBlock) k_due_scan(Dev<OffT> d, ClusterTables 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_emit_sched(Dev<OffT> d, const uint32_t* act, uint64_t* keys,
                                                        uint32_t* vals, uint64_t* best) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t k = d.ctr->n_clusters;
@@ -129,10 +130,55 @@ __global__ void __launch_bounds__(kBlock) k_emit_sched(Dev<OffT> d, const uint32
         }
 }
 
+// After the due scan: a round in which no cluster is due only walks.
+template <typename OffT>
+__global__ void k_walk_only_check(Dev<OffT> d) {
+    d.ctr->walk_only = (d.ctr->n_sweep == 0 && d.ctr->n_active > 0) ? 1u : 0u;
+}
+
+// A round that only walked: every cluster, label, row and list stays; the
+// next round's buffers take copies and every skip counter goes down by one.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_carry_all(Dev<OffT> d, ClusterTables t, ClusterTables nt,
+                                                      const uint32_t* act, uint32_t* act_next, const uint32_t* ids,
+                                                      uint32_t* ids_next) {
+    if (!d.ctr->walk_only) return;
+    const uint32_t k = d.ctr->n_clusters;
+    const uint32_t na = d.ctr->n_active;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t c = tid; c < k; c += stride) {
+        nt.start[c] = t.start[c];
+        nt.size[c] = t.size[c];
+        nt.vol[c] = t.vol[c];
+        nt.vol_start[c] = t.vol_start[c];
+        nt.root[c] = t.root[c];
+        nt.best[c] = ~0ull;
+        const uint16_t sk = t.skip[c];
+        nt.skip[c] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+        nt.hist[c] = t.hist[c];
+        if (d.trace) {
+            pxr_cluster_record& o = static_cast<pxr_cluster_record*>(d.records)[c];
+            o.origin = kOriginCarried;
+            o.skip = nt.skip[c];
+            o.round = d.ctr->rounds;
+        }
+    }
+    for (uint32_t i = tid; i < na; i += stride) {
+        act_next[i] = act[i];
+        ids_next[i] = ids[i];
+    }
+    if (tid == 0) {
+        d.ctr->n_keep = k;
+        d.ctr->n_active_next = na;
+    }
+}
+
 // Carried clusters: register their roots for the relabelling with data that
 // keeps them (count = size, spread 2, sum 0).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTables t, uint32_t* roots) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     for (uint32_t c0 = blockIdx.x * blockDim.x; c0 < k; c0 += gridDim.x * blockDim.x) {
         const uint32_t c = c0 + threadIdx.x;
@@ -159,6 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTabl
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_carry_vertices(Dev<OffT> d, ClusterTables t, const uint32_t* act,
                                                            uint32_t* act_next) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_active;
@@ -207,6 +254,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_vertices(Dev<OffT> d, ClusterT
 // were already handled by k_relabel (counter decremented, history kept).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock, 1) k_schedule(Dev<OffT> d, ClusterTables t, ClusterTables nt) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ float img[kMlpImage];
     if (d.sched)
         for (int p = threadIdx.x; p < kMlpImage; p += blockDim.x) img[p] = d.mlp[p];
