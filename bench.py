@@ -332,7 +332,8 @@ def product_arm(args, rank, world, local_rank):
     total_phase = sum(p["ms"] for p in phases)
     roofline = {
         "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
-        "kernel": {"walk": "k_walk", "sort": "sort_pass_kernel<u64> (time includes histogram, plan)"}[dom],
+        "kernel": {"walk": "k_walk (+ warp/CTA long-row kernels)",
+                   "sort": "sweep sort: sort_pass_kernel<u64> passes and k_chunk_sort (time includes histogram, plan)"}[dom],
         "algorithmic_bytes_per_launch": alg_total / units, "launches": units,
         "device_ms": by[dom]["ms"], "device_us_per_launch": 1e3 * by[dom]["ms"] / units,
         "traffic_source": "profiles/traffic.json: ncu DRAM bytes of full-size round-1 launches, scaled by items",

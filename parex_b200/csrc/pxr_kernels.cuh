@@ -165,6 +165,10 @@ __global__ void k_round_prep(Dev<OffT> d, int stage) {
         // every previous cluster fits a chunk: sort in shared memory (pxr_chunk.cuh)
         c->chunk_path = (!d.sched && c->max_parent <= kChunkCapRows && c->n_active > 0) ? 1u : 0u;
         c->n_gsort = c->chunk_path ? 0u : c->n_sweep;
+        if (c->chunk_path) {   // the chunked sort reads and writes every item once
+            c->stat_sort_items += c->n_sweep;
+            c->stat_sort_passes += 1;
+        }
     }
     if (stage == 2) c->max_csize_next = 0;
     const uint32_t k = c->n_clusters;
