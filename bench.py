@@ -54,20 +54,28 @@ WORKLOADS = {
     "rmat22": "R-MAT scale 22, edge factor 16, (a,b,c)=(0.57,0.19,0.19), seed 1, built on the GPU",
     "rmat24": "R-MAT scale 24, edge factor 16, (a,b,c)=(0.57,0.19,0.19), seed 1, built on the GPU",
     "regular22": "random 8-regular graph on 2^22 vertices, seed 1 (the no-split case)",
+    "batch512": ("512 planted-partition instances in one batched decomposition: n log-uniform in [1e3, 1e6], "
+                 "blocks U{2..64}, intra degree U[4, 32], inter degree U[0.1, 2], int64 offsets, built on the GPU"),
 }
 
 
 def load_workload(name, dev=None):
-    """(CSRGraph or None, device offsets, device cols, n, m) for a named workload."""
+    """(CSRGraph or None, device offsets, device cols, n, m, instance starts or
+    None) for a named workload."""
     from parex_b200 import graphs as G
     if name.startswith("rmat"):
-        import torch
         from parex_b200 import gpu_build as B
         off_d, cols_d, n, m = B.rmat(int(name[4:]), 16, seed=1, device=dev.index or 0)
-        return None, off_d, cols_d, n, m
+        return None, off_d, cols_d, n, m, None
+    if name == "batch512":
+        import torch
+        from parex_b200 import gpu_build as B
+        off_d, cols_d, n, m, starts = B.sbm_batch(512, seed=1, device=dev.index or 0)
+        return None, off_d.to(torch.int64), cols_d, n, m, starts
     g = {"grid128": lambda: G.grid3d(SIDE), "sbm16k": lambda: G.sbm_graph(),
          "regular22": lambda: G.random_regular(1 << 22, 8, seed=1)}[name]()
-    return g, None, None, g.n, g.m
+    return g, None, None, g.n, g.m, None
+
 
 
 def workload_config(g, extra=None, name="grid128"):
@@ -208,7 +216,8 @@ def product_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    g, off_d, cols_d, n, m = load_workload(args.workload, dev)
+    g, off_d, cols_d, n, m, starts = load_workload(args.workload, dev)
+    off64 = off_d is not None and off_d.dtype == torch.int64
     stream = torch.cuda.Stream(device=dev)
     if g is not None:
         off_d = torch.from_numpy(g.offsets.view(np.int32)).to(dev)
@@ -218,7 +227,7 @@ def product_arm(args, rank, world, local_rank):
     else:
         off_h = off_d.cpu().pin_memory()
         cols_h = cols_d.cpu().pin_memory()
-    off_hn = off_h.numpy().view(np.uint32)
+    off_hn = off_h.numpy().view(np.uint64 if off64 else np.uint32)
     cols_hn = cols_h.numpy().view(np.uint32)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
@@ -242,8 +251,20 @@ def product_arm(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
+    def init_device(dmx):
+        if starts is not None:
+            dmx.initialize_batched_device(n, m, off_d.data_ptr(), off64, cols_d.data_ptr(), starts)
+        else:
+            dmx.initialize_device(n, m, off_d.data_ptr(), off64, cols_d.data_ptr())
+
+    def init_host(dmx):
+        if starts is not None:
+            dmx.initialize_batched((off_hn, cols_hn), starts)
+        else:
+            dmx.initialize((off_hn, cols_hn))
+
     def device_step():
-        dm.initialize_device(n, m, off_d.data_ptr(), False, cols_d.data_ptr())
+        init_device(dm)
         return dm.expanderDecomposition()
 
     with torch.cuda.stream(stream):
@@ -279,7 +300,7 @@ def product_arm(args, rank, world, local_rank):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            dm.initialize((off_hn, cols_hn))
+            init_host(dm)
             dm.expanderDecomposition()
             fp_e2e = dm.getFinalPartition()
             e1.record(stream)
@@ -291,7 +312,7 @@ def product_arm(args, rank, world, local_rank):
         # per-phase device times with the stream driver (roofline)
         prof = manager(P.DRIVER_STREAM)
         prof.set_stream(stream.cuda_stream)
-        prof.initialize_device(n, m, off_d.data_ptr(), False, cols_d.data_ptr())
+        init_device(prof)
         prof.set_profiling(True)
         prof.expanderDecomposition()
         phases = prof.phase_stats()
@@ -307,7 +328,7 @@ def product_arm(args, rank, world, local_rank):
         return 0
     value = m * world * args.steps / (total_ms / 1e3)
     e2e_value = m * world * args.steps / (e2e_ms / 1e3)
-    h2d = (n + 1) * 4 + 2 * m * 4
+    h2d = (n + 1) * (8 if off64 else 4) + 2 * m * 4
     d2h = n * 4 + 4
 
     # roofline of the dominant phase among those with algorithmic byte counts;
@@ -353,7 +374,8 @@ def product_arm(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config((n, m), {"driver": "cuda graph, device-driven round loop", "rounds": rounds,
                                            "clusters": clusters, "cut_edges_device": device_cut,
-                                           "sweep_schedule": args.schedule, "row_plan": dm.row_plan()},
+                                           "sweep_schedule": args.schedule, "row_plan": dm.row_plan(),
+                                           "instances": None if starts is None else int(len(starts) - 1)},
                                   args.workload),
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -232,6 +232,12 @@ pxr_status pxr_get_row_plan(pxr_handle* h, pxr_row_plan* out);
  * Applied at once when a graph is loaded. */
 pxr_status pxr_set_row_plan(pxr_handle* h, const pxr_row_plan* plan);
 
+/* pxr_initialize_batched with the CSR in device memory (offsets 64-bit when
+ * offsets_are_64bit, else 32-bit); instance_start stays a host array. */
+pxr_status pxr_initialize_batched_device(pxr_handle* h, uint32_t n, uint64_t m, const void* offsets,
+                                         int offsets_are_64bit, const uint32_t* cols, uint32_t n_instances,
+                                         const uint32_t* instance_start);
+
 /* CudaDeviceManager::iterateRandomWalk() (cuda/interface.h:29). */
 pxr_status pxr_walk_step(pxr_handle* h);
 /* CudaDeviceManager::computeSweepCuts() (cuda/interface.h:32). */
@@ -328,6 +334,26 @@ pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* a
 size_t pxr_build_csr_scratch_bytes(uint64_t n_edges);
 pxr_status pxr_build_csr(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
                          uint32_t* offsets, uint32_t* cols, uint64_t* m_out, void* stream);
+/* One block pair of a planted-partition instance: candidate pairs
+ * (base_u + i, base_v + j), i < su, j < sv (intra: i < j < su, base_u == base_v),
+ * each an edge with probability p. */
+typedef struct {
+    uint32_t base_u, base_v, su, sv;
+    double p;
+    uint32_t intra;
+    uint32_t reserved;
+} pxr_sbm_task;
+/* Planted-partition edges on the device by geometric skipping: the candidate
+ * range of task t is cut into segments of segment_len candidates;
+ * seg_prefix[t] is the first global segment of task t (n_tasks + 1 entries,
+ * ending with n_segments).  Two calls, all arrays in device memory: with
+ * seg_offset == NULL the number of edges of every segment goes to
+ * seg_count[n_segments]; then, with seg_offset the exclusive prefix of those
+ * counts, the edges go to u, v (segment by segment, in candidate order).
+ * Deterministic in seed; pxr_build_csr turns the list into the CSR. */
+pxr_status pxr_sbm_edges(const pxr_sbm_task* tasks, uint32_t n_tasks, const uint64_t* seg_prefix, uint64_t n_segments,
+                         uint64_t segment_len, uint64_t seed, uint32_t* seg_count, const uint64_t* seg_offset,
+                         uint32_t* u, uint32_t* v, void* stream);
 /* R-MAT edge samples on the device: samples (u, v) pairs over 2^scale
  * vertices, quadrant probabilities a, b, c (d = 1 - a - b - c), from the
  * counter-based hash of parex_b200/graphs.py rmat() (same seed, same edges). */

@@ -32,7 +32,7 @@ SYMBOLS = [
     "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
     "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
-    "pxr_rmat_edges",
+    "pxr_rmat_edges", "pxr_sbm_edges", "pxr_initialize_batched_device",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -87,6 +87,10 @@ class ClusterRecord(C.Structure):
                 ("prev_sparsity", C.c_float), ("prev_round", C.c_uint32), ("age", C.c_uint32),
                 ("round", C.c_uint32), ("skip", C.c_uint32), ("prediction", C.c_float), ("has_prev", C.c_uint32),
                 ("reserved", C.c_uint32 * 2), ("features", C.c_float * MLP_FEATURES)]
+
+
+SBM_TASK_DTYPE = np.dtype([("base_u", "<u4"), ("base_v", "<u4"), ("su", "<u4"), ("sv", "<u4"), ("p", "<f8"),
+                           ("intra", "<u4"), ("reserved", "<u4")])
 
 
 class MlpLoss(C.Structure):
@@ -166,6 +170,8 @@ def load() -> C.CDLL:
     L.pxr_build_csr_scratch_bytes.argtypes = [u64]
     L.pxr_build_csr.argtypes = [u32, u64, p, p, p, p, p, C.POINTER(u64), p]
     L.pxr_rmat_edges.argtypes = [u32, u64, C.c_double, C.c_double, C.c_double, u64, p, p, p]
+    L.pxr_sbm_edges.argtypes = [p, u32, p, u64, u64, u64, p, p, p, p, p]
+    L.pxr_initialize_batched_device.argtypes = [p, u32, u64, p, C.c_int, p, u32, p]
     L.pxr_set_row_plan.argtypes = [p, C.POINTER(RowPlan)]
     L.pxr_read_cluster_records.argtypes = [p, p, u32, C.POINTER(u32)]
     L.pxr_mlp_forward.argtypes = [p, u32, p, p, p, p]

@@ -100,6 +100,70 @@ __global__ void k_csr_rows(const uint64_t* sorted0, const uint64_t* sorted1, con
     }
 }
 
+// Planted-partition edges by geometric skipping: one thread per segment of a
+// block pair's candidate range; a segment restarts the skipping (the gaps
+// are memoryless).  Candidate k of an inter-block pair is (k / sv, k % sv);
+// of an intra-block pair the k-th (row, col) with row < col in row order.
+__device__ __forceinline__ double uniform_open(uint64_t& state) {
+    state = splitmix64(state);
+    return ((double)(state >> 11) + 1.0) * (1.0 / 9007199254740992.0);   // (0, 1]
+}
+
+__device__ __forceinline__ void tri_unrank(uint64_t k, uint64_t s, uint64_t* r, uint64_t* c) {
+    // row r holds s - 1 - r candidates and starts at r (2s - r - 1) / 2
+    const double b = 2.0 * (double)s - 1.0;
+    int64_t row = (int64_t)((b - sqrt(b * b - 8.0 * (double)k)) / 2.0);
+    if (row < 0) row = 0;
+    auto start = [&](int64_t q) { return (uint64_t)q * (2 * s - (uint64_t)q - 1) / 2; };
+    while (row > 0 && start(row) > k) --row;
+    while ((uint64_t)row + 1 < s && start(row + 1) <= k) ++row;
+    *r = (uint64_t)row;
+    *c = k - start(row) + (uint64_t)row + 1;
+}
+
+__global__ void k_sbm_segments(const pxr_sbm_task* tasks, uint32_t n_tasks, const uint64_t* seg_prefix,
+                               uint64_t n_segments, uint64_t seg_len, uint64_t seed, uint32_t* seg_count,
+                               const uint64_t* seg_offset, uint32_t* u, uint32_t* v) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n_segments;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n_tasks;   // task: last t with seg_prefix[t] <= g
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (seg_prefix[mid] <= g) lo = mid; else hi = mid;
+        }
+        const pxr_sbm_task tk = tasks[lo];
+        const uint64_t su = tk.su, sv = tk.sv;
+        const uint64_t total = tk.intra ? su * (su - 1) / 2 : su * sv;
+        const uint64_t k0 = (g - seg_prefix[lo]) * seg_len;
+        const uint64_t k1 = min(total, k0 + seg_len);
+        uint32_t drawn = 0;
+        const uint64_t out = seg_offset ? seg_offset[g] : 0;
+        if (tk.p > 0.0 && k0 < k1) {
+            uint64_t state = splitmix64(seed ^ splitmix64(g * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull));
+            const double lq = log1p(-min(tk.p, 1.0 - 1e-16));
+            uint64_t k = k0;
+            bool first = true;
+            for (;;) {
+                const double skip = floor(log(uniform_open(state)) / lq);
+                if (!(skip < 1e18)) break;
+                const uint64_t step = (uint64_t)skip + (first ? 0 : 1);
+                first = false;
+                if (step >= k1 - k) break;
+                k += step;
+                if (seg_offset) {
+                    uint64_t a, b;
+                    if (tk.intra) tri_unrank(k, su, &a, &b);
+                    else { a = k / sv; b = k % sv; }
+                    u[out + drawn] = tk.base_u + (uint32_t)a;
+                    v[out + drawn] = tk.base_v + (uint32_t)b;
+                }
+                ++drawn;
+            }
+        }
+        if (!seg_offset) seg_count[g] = drawn;
+    }
+}
+
 __global__ void k_set_u32(uint32_t* p, uint32_t value) { *p = value; }
 
 struct BuildLayout {
@@ -146,6 +210,18 @@ pxr_status pxr_rmat_edges(uint32_t scale, uint64_t samples, double a, double b, 
     const uint64_t blocks = std::min<uint64_t>((samples + kBuildBlock - 1) / kBuildBlock, 148u * 32u);
     k_rmat<<<(uint32_t)blocks, kBuildBlock, 0, static_cast<cudaStream_t>(stream)>>>(samples, scale, ta, tab, tabc,
                                                                                     seed, u, v);
+    return cudaGetLastError() == cudaSuccess ? PXR_OK : PXR_CUDA_ERROR;
+}
+
+pxr_status pxr_sbm_edges(const pxr_sbm_task* tasks, uint32_t n_tasks, const uint64_t* seg_prefix, uint64_t n_segments,
+                         uint64_t segment_len, uint64_t seed, uint32_t* seg_count, const uint64_t* seg_offset,
+                         uint32_t* u, uint32_t* v, void* stream) {
+    if (!tasks || !seg_prefix || segment_len == 0 || n_tasks == 0) return PXR_INVALID_ARG;
+    if (seg_offset ? (!u || !v) : !seg_count) return PXR_INVALID_ARG;
+    if (!n_segments) return PXR_OK;
+    const uint64_t blocks = std::min<uint64_t>((n_segments + kBuildBlock - 1) / kBuildBlock, 148u * 64u);
+    k_sbm_segments<<<(uint32_t)blocks, kBuildBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+        tasks, n_tasks, seg_prefix, n_segments, segment_len, seed, seg_count, seg_offset, u, v);
     return cudaGetLastError() == cudaSuccess ? PXR_OK : PXR_CUDA_ERROR;
 }
 

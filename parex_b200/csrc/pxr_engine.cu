@@ -1266,6 +1266,29 @@ pxr_status pxr_initialize_batched(pxr_handle* h, uint32_t n, uint64_t m, const u
     return batch_setup<uint64_t>(h, n_instances, instance_start);
 }
 
+pxr_status pxr_initialize_batched_device(pxr_handle* h, uint32_t n, uint64_t m, const void* offsets,
+                                         int offsets_are_64bit, const uint32_t* cols, uint32_t n_instances,
+                                         const uint32_t* instance_start) {
+    if (!h) return PXR_INVALID_ARG;
+    if (!instance_start || n_instances == 0) return fail(h, PXR_INVALID_ARG, "no instances");
+    if (instance_start[0] != 0 || instance_start[n_instances] != n)
+        return fail(h, PXR_INVALID_ARG, "instance starts must run from 0 to n");
+    for (uint32_t i = 0; i < n_instances; ++i)
+        if (instance_start[i + 1] <= instance_start[i])
+            return fail(h, PXR_INVALID_ARG, "every instance needs at least one vertex");
+    pxr_status st;
+    if (offsets_are_64bit) {
+        st = initialize_impl<uint64_t>(h, n, m, static_cast<const uint64_t*>(offsets), cols, cudaMemcpyDeviceToDevice,
+                                       true);
+        if (st != PXR_OK) return st;
+        return batch_setup<uint64_t>(h, n_instances, instance_start);
+    }
+    if (2 * m >= (1ull << 32)) return fail(h, PXR_INVALID_ARG, "32-bit offsets need 2m < 2^32");
+    st = initialize_impl<uint32_t>(h, n, m, static_cast<const uint32_t*>(offsets), cols, cudaMemcpyDeviceToDevice, true);
+    if (st != PXR_OK) return st;
+    return batch_setup<uint32_t>(h, n_instances, instance_start);
+}
+
 pxr_status pxr_walk_step(pxr_handle* h) { return run_op(h, kOpWalk); }
 pxr_status pxr_sweep(pxr_handle* h) { return run_op(h, kOpSweep); }
 pxr_status pxr_cut_clusters(pxr_handle* h) { return run_op(h, kOpCut); }

@@ -67,3 +67,79 @@ def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c:
 
 def to_host(offsets, cols, name: str = "") -> CSRGraph:
     return CSRGraph(offsets.cpu().numpy().view(np.uint32).copy(), cols.cpu().numpy().view(np.uint32).copy(), name)
+
+
+def sbm_batch_params(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 1e6, scale: float = 1.0):
+    """Per-instance (n, blocks, d_in, d_out), drawn as graphs.sbm_batch draws them."""
+    import math
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng([seed, i])
+        n = max(4, int(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi))) * scale))
+        blocks = int(rng.integers(2, 65))
+        blocks = min(blocks, max(1, n // 2))
+        d_in = float(rng.uniform(4, 32))
+        d_out = float(rng.uniform(0.1, 2))
+        out.append((n, blocks, d_in, d_out))
+    return out
+
+
+def sbm_batch(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 1e6, scale: float = 1.0,
+              device: int = 0, segment_len: int = 1 << 24):
+    """Disjoint union of planted-partition instances built on the device:
+    (offsets, cols, n, m, instance_start).  Instance parameters as
+    graphs.sbm_batch; edges drawn on the device (pxr_sbm_edges), so the edge
+    sample differs from the host generator's while following the same
+    distribution (Bernoulli pairs, p_in = d_in / (b - 1), p_out = d_out / (n - b))."""
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda", device)
+    params = sbm_batch_params(count, seed, n_lo, n_hi, scale)
+    tasks = []
+    starts = [0]
+    for n, blocks, d_in, d_out in params:
+        base = starts[-1]
+        bsz = n // blocks
+        sizes = [bsz] * blocks
+        sizes[-1] += n - bsz * blocks
+        bstart = np.concatenate([[0], np.cumsum(sizes)]) + base
+        p_in = d_in / max(bsz - 1, 1)
+        p_out = d_out / max(n - bsz, 1)
+        for a in range(blocks):
+            tasks.append((bstart[a], bstart[a], sizes[a], sizes[a], min(p_in, 1.0), 1))
+            for b in range(a + 1, blocks):
+                tasks.append((bstart[a], bstart[b], sizes[a], sizes[b], min(p_out, 1.0), 0))
+        starts.append(base + n)
+    T = np.zeros(len(tasks), dtype=_lib.SBM_TASK_DTYPE)
+    arr = np.asarray(tasks, dtype=np.float64)
+    T["base_u"], T["base_v"] = arr[:, 0], arr[:, 1]
+    T["su"], T["sv"], T["p"], T["intra"] = arr[:, 2], arr[:, 3], arr[:, 4], arr[:, 5]
+    su, sv = T["su"].astype(np.uint64), T["sv"].astype(np.uint64)
+    cand = np.where(T["intra"] == 1, su * (su - np.uint64(1)) // np.uint64(2), su * sv)
+    nseg = (cand + np.uint64(segment_len - 1)) // np.uint64(segment_len)
+    prefix = np.zeros(len(tasks) + 1, dtype=np.uint64)
+    np.cumsum(nseg, out=prefix[1:])
+    n_segments = int(prefix[-1])
+    d_tasks = torch.from_numpy(T.view(np.uint8).copy()).to(dev)
+    d_prefix = torch.from_numpy(prefix.view(np.int64).copy()).to(dev)
+    d_count = torch.zeros(max(n_segments, 1), dtype=torch.int32, device=dev)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    st = L.pxr_sbm_edges(_p(d_tasks), len(tasks), _p(d_prefix), n_segments, segment_len, seed, _p(d_count), None,
+                         None, None, stream)
+    if st != 0:
+        raise _lib.PxrError(st, "pxr_sbm_edges (count)")
+    counts = d_count[:n_segments].to(torch.int64)
+    offs = torch.zeros(max(n_segments, 1), dtype=torch.int64, device=dev)
+    if n_segments > 1:
+        offs[1:n_segments] = torch.cumsum(counts, 0)[:-1]
+    total = int(counts.sum().item()) if n_segments else 0
+    u = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+    v = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+    st = L.pxr_sbm_edges(_p(d_tasks), len(tasks), _p(d_prefix), n_segments, segment_len, seed, None, _p(offs),
+                         _p(u), _p(v), stream)
+    if st != 0:
+        raise _lib.PxrError(st, "pxr_sbm_edges (write)")
+    del d_count, offs
+    n_total = starts[-1]
+    offsets, cols, m = build_csr(n_total, u[:total], v[:total], device)
+    return offsets, cols, n_total, m, np.asarray(starts, dtype=np.uint32)

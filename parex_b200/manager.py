@@ -127,6 +127,14 @@ class CudaDeviceManager:
                    _ptr(starts))
         self.n, self.m = n, m
 
+    def initialize_batched_device(self, n: int, m: int, offsets_ptr: int, offsets_are_64bit: bool, cols_ptr: int,
+                                  instance_start) -> None:
+        """initialize_batched() from a CSR already in device memory."""
+        starts = np.ascontiguousarray(instance_start, dtype=np.uint32)
+        self._call(self._L.pxr_initialize_batched_device, n, m, C.c_void_p(offsets_ptr), 1 if offsets_are_64bit else 0,
+                   C.c_void_p(cols_ptr), int(starts.shape[0] - 1), _ptr(starts))
+        self.n, self.m = n, m
+
     def iterateRandomWalk(self) -> None:
         self._call(self._L.pxr_walk_step)
 

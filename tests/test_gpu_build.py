@@ -68,3 +68,29 @@ def test_device_csr_decomposes_like_host_csr():
     b.initialize(G.rmat(13, 16, seed=2))
     b.expanderDecomposition()
     np.testing.assert_array_equal(a.getFinalPartition().clusterIds, b.getFinalPartition().clusterIds)
+
+
+def test_device_sbm_batch_structure_and_decomposition():
+    off, cols, n, m, starts = B.sbm_batch(count=10, seed=3, n_lo=200, n_hi=6000, segment_len=1 << 12)
+    off2, cols2, n2, m2, starts2 = B.sbm_batch(count=10, seed=3, n_lo=200, n_hi=6000, segment_len=1 << 12)
+    g = B.to_host(off, cols)
+    np.testing.assert_array_equal(g.cols, B.to_host(off2, cols2).cols)     # deterministic in the seed
+    np.testing.assert_array_equal(starts, starts2)
+    inst = np.repeat(np.arange(starts.shape[0] - 1), np.diff(starts.astype(np.int64)))
+    src = np.repeat(np.arange(n), np.diff(g.offsets.astype(np.int64)))
+    assert np.all(inst[src] == inst[g.cols])                                  # no edge leaves its instance
+    params = B.sbm_batch_params(count=10, seed=3, n_lo=200, n_hi=6000)
+    for i, (ni, blocks, d_in, d_out) in enumerate(params):
+        if ni < 2000:
+            continue
+        lo, hi = int(starts[i]), int(starts[i + 1])
+        mean = (g.offsets[hi] - g.offsets[lo]) / ni
+        assert abs(mean - (d_in + d_out)) < 0.1 * (d_in + d_out) + 0.5, (i, mean, d_in + d_out)
+    # the device-built batch decomposes the same from device and host arrays
+    a = P.CudaDeviceManager()
+    a.initialize_batched_device(n, m, off.data_ptr(), False, cols.data_ptr(), starts)
+    a.expanderDecomposition()
+    b = P.CudaDeviceManager()
+    b.initialize_batched(g, starts)
+    b.expanderDecomposition()
+    np.testing.assert_array_equal(a.getFinalPartition().clusterIds, b.getFinalPartition().clusterIds)
