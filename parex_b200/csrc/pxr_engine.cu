@@ -18,6 +18,10 @@ using namespace pxr;
 
 namespace pxr {
 constexpr uint32_t kMaxGrid = 148u * 32u;
+#ifndef PXR_UNION_LANES
+#define PXR_UNION_LANES 1
+#endif
+constexpr int kUnionLanes = PXR_UNION_LANES;   // lanes per light row in k_union
 
 // ---------------------------------------------------------------------------
 // final partition on the device (PartitionManager::finalizePartition,
@@ -268,12 +272,12 @@ struct pxr_handle {
     uint8_t* split = nullptr;
     pxr_sweep_cut* allcuts = nullptr;
     uint32_t* roots[2] = {nullptr, nullptr};
-    LookbackState lb[kSiteCarry + 1]{};
+    LookbackState lb[kSiteRoots + 1]{};
+    uint32_t* rootmap = nullptr;
     uint32_t* lb_epoch = nullptr;
     RoundCtr* ctr = nullptr;
     SortState sort{};
     uint32_t* sort_end_bit = nullptr;
-    uint32_t* root_end_bit = nullptr;
     uint32_t* fp_end_bit = nullptr;
     uint32_t* d_n = nullptr;
     int32_t* d_num = nullptr;
@@ -398,7 +402,6 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.ctr = h->ctr;
     d.sort = h->sort;
     d.sort_end_bit = h->sort_end_bit;
-    d.root_end_bit = h->root_end_bit;
     d.light_max = h->light_max;
     d.wide = h->wide;
     d.n_wide = h->n_wide;
@@ -412,6 +415,9 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.lb_sched = h->lb[kSiteSched];
     d.lb_emit = h->lb[kSiteEmit];
     d.lb_carry = h->lb[kSiteCarry];
+    d.lb_roots = h->lb[kSiteRoots];
+    d.rootmap = h->rootmap;
+    d.n_words = (h->n + 31u) / 32u;
     d.mlp = h->mlp;
     d.safety = h->sched.safety;
     d.max_skip = h->sched.max_skip;
@@ -555,36 +561,25 @@ cudaError_t op_cut(pxr_handle* h) {
         phase(h, kPhSched, 2, [&] {
             k_carry_all<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, nt, h->act[h->acur], h->act[h->acur ^ 1],
                                                                  h->ids[h->acur], h->ids[h->acur ^ 1]);
-            k_carry_roots<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->roots[0]);
+            k_carry_roots<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t);
         });
     phase(h, kPhCutInit, 1, [&] {
         k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });
     phase(h, kPhUnion, 3 + long_launches(h), [&] {
-        k_link_first<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
-        k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
-        k_union<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->vals[0], h->vals[1], h->keys[0],
-                                                                           h->keys[1]);
+        k_link_first<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        k_union<OffT, kUnionLanes><<<grid_for((uint64_t)h->n * kUnionLanes), kBlock, 0, s>>>(d, h->ids[h->acur]);
         PXR_LONG(h, k_union_long, d);
     });
     phase(h, kPhComponents, 1, [&] {
         k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1],
-                                                                              h->keys[0], h->keys[1], h->roots[0]);
+                                                                              h->keys[0], h->keys[1]);
     });
-    SortBuffers<uint32_t> rb{};
-    rb.keys[0] = h->roots[0]; rb.keys[1] = h->roots[1];
-    rb.count = &h->ctr->n_roots;
-    rb.end_bit = h->root_end_bit;
-    rb.capacity = h->n;
-    cudaError_t e = cudaSuccess;
-    const int root_bits = (int)std::max(1u, host_bitlen(h->n));
-    phase(h, kPhRootSort, 2 + (root_bits + 7) / 8, [&] {
-        SortState rs = h->sort;
-        rs.items_moved = nullptr;
-        e = radix_sort<uint32_t>(rb, rs, &h->ctr->err, s, root_bits);
-    });
-    if (e != cudaSuccess) return e;
-    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], h->roots[1], t, nt); });
+    // roots in vertex-id order (the order of the reference's root sort)
+    const uint32_t root_tiles = (uint32_t)(((h->n + 31u) / 32u + kRootTileWords - 1) / kRootTileWords);
+    phase(h, kPhRootSort, 1, [&] { k_root_compact<OffT><<<std::max(root_tiles, 1u), kBlock, 0, s>>>(d, h->roots[0]); });
+    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], t, nt); });
     if (h->sched.mode)
         phase(h, kPhSched, 1, [&] {
             k_carry_vertices<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->act[h->acur], h->act[h->acur ^ 1]);
@@ -800,14 +795,15 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->sflag, N); A(&h->nflag, N); A(&h->rootc, N); A(&h->mlp, (size_t)kMlpImage);
     if (h->sched.trace) { A(&h->records, N); }
     A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N);
-    for (int i = 0; i <= kSiteCarry; ++i) {
+    for (int i = 0; i <= kSiteRoots; ++i) {
         A(&h->lb[i].flags, scan_tiles); A(&h->lb[i].agg, scan_tiles); A(&h->lb[i].inc, scan_tiles);
     }
+    A(&h->rootmap, N / 32 + 1);
     A(&h->lb_epoch, kSites); A(&h->ctr, 1);
     A(&h->sort.hist, kMaxPasses * kRadix); A(&h->sort.bases, kMaxPasses * kRadix);
     A(&h->sort.pass_info, kMaxPasses + 1); A(&h->sort.tile_ctr, kMaxPasses); A(&h->sort.epoch, 1);
     A(&h->sort.status, (size_t)sort_tiles * kRadix);
-    A(&h->sort_end_bit, 1); A(&h->root_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
+    A(&h->sort_end_bit, 1); A(&h->fp_end_bit, 1); A(&h->d_n, 1);
     A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 4); A(&h->heavy, N); A(&h->wide, N);
     A(&h->probe_ctr, 1); A(&h->hist, 33);
 #undef A
@@ -817,7 +813,8 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     // look-back flags and sort status words carry epochs that only grow, so
     // they are cleared once here and never again
     cudaStream_t s = h->stream;
-    for (int i = 0; i <= kSiteCarry; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
+    for (int i = 0; i <= kSiteRoots; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->rootmap, 0, (N / 32 + 1) * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, kSites * 4, s));
     h->records_n = h->records ? (uint32_t)N : 0u;
     if (!h->mlp_img.empty())
@@ -827,10 +824,9 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     PXR_CUDA(h, cudaMemsetAsync(h->sort.epoch, 0, 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.status, 0, (size_t)sort_tiles * kRadix * 8, s));
     PXR_CUDA(h, cudaMemsetAsync(h->sort.pass_info, 0, (kMaxPasses + 1) * 4, s));
-    const uint32_t consts[3] = {host_bitlen(n > 0 ? n - 1 : 0), 32u, n};
-    PXR_CUDA(h, cudaMemcpyAsync(h->root_end_bit, &consts[0], 4, cudaMemcpyHostToDevice, s));
-    PXR_CUDA(h, cudaMemcpyAsync(h->fp_end_bit, &consts[1], 4, cudaMemcpyHostToDevice, s));
-    PXR_CUDA(h, cudaMemcpyAsync(h->d_n, &consts[2], 4, cudaMemcpyHostToDevice, s));
+    const uint32_t consts[2] = {32u, n};
+    PXR_CUDA(h, cudaMemcpyAsync(h->fp_end_bit, &consts[0], 4, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemcpyAsync(h->d_n, &consts[1], 4, cudaMemcpyHostToDevice, s));
     return PXR_OK;
 }
 

@@ -481,12 +481,15 @@ __global__ void __launch_bounds__(kBlock) k_cut_init(Dev<OffT> d, ClusterTables 
         const uint32_t co = d.cut_off[c];
         const uint32_t pos = i - t.start[c] + 1u;
         d.lab[v] = (co != kNoCut && pos > co) ? (int32_t)(k + c) : (int32_t)c;
-        d.parent[v] = v;
-        d.acc_max[v] = 0u;
-        d.acc_min[v] = 0xFFFFFFFFu;
-        d.acc_sum[v] = 0;
-        d.acc_cnt[v] = 0u;
     }
+}
+
+// cluster a vertex belonged to this round, or k when it is not in a split
+// cluster (after k_cut_init, labels of a split cluster c are c or k + c)
+template <typename OffT>
+__device__ __forceinline__ bool in_split(const Dev<OffT>& d, uint32_t k, int32_t lv) {
+    const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;
+    return lv >= 0 && c < k && d.split[c];
 }
 
 // Every parent pointer points to a smaller id (roots are hooked under smaller
@@ -504,88 +507,106 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t v) {
     return v;
 }
 
+// The three linking kernels walk this round's active list in vertex order
+// (the walk's list), so rows, labels and parent words of neighbouring ids are
+// read together; the forest they build does not depend on the order.
+//
 // First linking pass: each vertex of a split cluster points to its smallest
-// same-label neighbour below it (rows are sorted, so the first one found).
-// Only the owning thread writes parent[v] here.
+// same-label neighbour below it (rows are sorted, so the first one found), or
+// to itself.  Only the owning thread writes parent[v] here; the vertex's
+// accumulators for the component data start from the identity.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
-                                                       const uint64_t* keys0, const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_sweep;
-    const uint32_t sel = d.ctr->main_sel;
-    const uint32_t* vals = sel ? vals1 : vals0;
-    const uint64_t* keys = sel ? keys1 : keys0;
+__global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32_t* ids) {
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
-        const uint32_t c = (uint32_t)(keys[j] >> 32);
-        if (!d.split[c]) continue;
-        const uint32_t v = vals[j];
+        const uint32_t v = ids[j];
         const int32_t lv = d.lab[v];
+        if (!in_split(d, k, lv)) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
+        uint32_t p = v;
         for (OffT s = beg; s < end; ++s) {
             const uint32_t nb = d.cols[s];
             if (nb == kInvalidEdge) continue;  // disabled slots keep their place in the sorted row
             if (nb >= v) break;                // no smaller neighbour left
-            if (d.lab[nb] == lv) { d.parent[v] = nb; break; }
+            if (d.lab[nb] == lv) { p = nb; break; }
         }
+        d.parent[v] = p;
+        d.acc_max[v] = 0u;
+        d.acc_min[v] = 0xFFFFFFFFu;
+        d.acc_sum[v] = 0;
+        d.acc_cnt[v] = 0u;
     }
 }
 
 // Flatten the linked forest: every vertex of a split cluster points at its root.
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
-                                                     const uint64_t* keys0, const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_sweep;
-    const uint32_t sel = d.ctr->main_sel;
-    const uint32_t* vals = sel ? vals1 : vals0;
-    const uint64_t* keys = sel ? keys1 : keys0;
+__global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t* ids) {
+    if (d.ctr->walk_only) return;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
-        const uint32_t c = (uint32_t)(keys[j] >> 32);
-        if (!d.split[c]) continue;
-        const uint32_t v = vals[j];
+        const uint32_t v = ids[j];
+        if (!in_split(d, k, d.lab[v])) continue;
         const uint32_t r = uf_find(d.parent, v);
         atomicMin(&d.parent[v], r);
     }
 }
 
+// Join the sets of v and nb (both in a split cluster, same label).  hint is
+// a word of v's set: when nb's parent is it, the two are joined already.
+__device__ __forceinline__ void uf_join(uint32_t* parent, uint32_t* err, uint32_t v, uint32_t nb, uint32_t& hint) {
+    if (ld_relaxed(&parent[nb]) == hint) return;
+    uint32_t a = v, b = nb;
+    for (uint32_t tries = 0;; ++tries) {
+        if (tries > kSpinLimit) { atomicOr(err, kErrUnionFind); return; }
+        const uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+        if (ra == rb) { hint = ra; return; }
+        const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+        if (atomicCAS(&parent[hi], hi, lo) == hi) { hint = lo; return; }
+        a = hi;
+        b = lo;
+    }
+}
+
 // union over same-label valid edges (ConsolidationManager::consolidate,
-// cuda/devConsolidate.h:46-112, 168-204), each undirected edge once.
+// cuda/devConsolidate.h:46-112, 168-204), each undirected edge once (from its
+// larger end; rows are sorted, so a lane stops at the first neighbour >= v).
 template <typename OffT, int W>
-__global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* vals0, const uint32_t* vals1,
-                                                  const uint64_t* keys0, const uint64_t* keys1) {
-    const uint32_t count = d.ctr->n_sweep;
-    const uint32_t sel = d.ctr->main_sel;
-    const uint32_t* vals = sel ? vals1 : vals0;
-    const uint64_t* keys = sel ? keys1 : keys0;
+__global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* ids) {
+    if (d.ctr->walk_only) return;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
     const uint32_t gl = threadIdx.x & (W - 1);
     const uint32_t groups = (gridDim.x * blockDim.x) / W;
     for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) / W; j < count; j += groups) {
-        const uint32_t c = (uint32_t)(keys[j] >> 32);
-        if (!d.split[c]) continue;
-        const uint32_t v = vals[j];
+        const uint32_t v = ids[j];
         const int32_t lv = d.lab[v];
+        if (!in_split(d, k, lv)) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
         if ((uint64_t)(end - beg) > d.light_max) continue;   // k_union_long
+        uint32_t hint = ld_relaxed(&d.parent[v]);
         for (OffT s = beg + gl; s < end; s += W) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
-            uint32_t a = v, b = nb;
-            for (uint32_t tries = 0;; ++tries) {
-                if (tries > kSpinLimit) { atomicOr(&d.ctr->err, kErrUnionFind); break; }
-                const uint32_t ra = uf_find(d.parent, a), rb = uf_find(d.parent, b);
-                if (ra == rb) break;
-                const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
-                if (atomicCAS(&d.parent[hi], hi, lo) == hi) break;
-                a = hi;
-                b = lo;
-            }
+            if (nb == kInvalidEdge) continue;
+            if (nb >= v) break;
+            if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
     }
+}
+
+// root registry: one bit per vertex id
+template <typename OffT>
+__device__ __forceinline__ void mark_root(const Dev<OffT>& d, uint32_t r) {
+    atomicOr(&d.rootmap[r >> 5], 1u << (r & 31u));
 }
 
 // roots, per-cluster data (computeClusterData, cuda/devPartition.h:380-411)
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                             const uint32_t* vals1, const uint64_t* keys0,
-                                                            const uint64_t* keys1, uint32_t* roots) {
+                                                            const uint64_t* keys1) {
     const uint32_t count = d.ctr->n_sweep;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
@@ -599,8 +620,6 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
         bool has = false, single = true;
         uint32_t k_first = 0, k_last = 0;
         ClusterAcc a_first = DataAgg::identity(), a_last = DataAgg::identity();
-        uint32_t my_roots[kScanItems];
-        uint32_t n_my = 0;
         for (int k = 0; k < kScanItems; ++k) {
             const uint32_t i = first + k;
             if (i >= count) break;
@@ -612,12 +631,12 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
                 r = uf_find(d.parent, v);
                 atomicMin(&d.parent[v], r);
                 if (r == v) {
-                    my_roots[n_my++] = r;
+                    mark_root(d, r);
                     d.rootc[r] = (kOriginChild << 30) | c;
                 }
             } else {
                 r = t.root[c];
-                if (i == t.start[c]) my_roots[n_my++] = r;
+                if (i == t.start[c]) mark_root(d, r);
             }
             const float xv = d.x[v];
             const uint32_t ob = ordered_bits(xv);
@@ -634,19 +653,56 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
                 a_last = cur;
             }
         }
-        // register this warp's roots with one atomic
-        uint32_t incl = n_my;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if ((threadIdx.x & 31u) >= (uint32_t)o) incl += u;
-        }
-        const uint32_t warp_total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        uint32_t slot = 0;
-        if ((threadIdx.x & 31u) == 31u && warp_total) slot = atomicAdd(&d.ctr->n_roots, warp_total);
-        slot = __shfl_sync(0xFFFFFFFFu, slot, 31) + incl - n_my;
-        for (uint32_t q = 0; q < n_my; ++q) roots[slot + q] = my_roots[q];
         emit_fragments<DataAgg>(has, single, k_first, a_first, k_last, a_last, agg);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// roots in vertex-id order: the root bitmap compacted with a decoupled
+// look-back over tiles of kRootWords words per thread; the words are cleared
+// as they are read, so the bitmap is zero again for the next round.
+
+constexpr int kRootWords = 4;
+constexpr uint32_t kRootTileWords = kBlock * kRootWords;
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_root_compact(Dev<OffT> d, uint32_t* roots) {
+    __shared__ uint64_t warp_tot[kBlock / 32];
+    __shared__ uint64_t s_excl;
+    if (d.ctr->walk_only) return;   // nothing due: the round only walks
+    const uint32_t nw = d.n_words;
+    const uint32_t ntiles = (nw + kRootTileWords - 1) / kRootTileWords;
+    const uint32_t tile = fetch_tile(d.ctr, kSiteRoots);
+    if (tile >= ntiles) return;
+    const uint32_t epoch = d.lb_epoch[kSiteRoots];
+    const uint32_t w0 = tile * kRootTileWords + threadIdx.x * kRootWords;
+    uint32_t words[kRootWords];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int q = 0; q < kRootWords; ++q) {
+        const uint32_t w = w0 + q;
+        words[q] = w < nw ? d.rootmap[w] : 0u;
+        if (words[q]) d.rootmap[w] = 0u;
+        cnt += __popc(words[q]);
+    }
+    uint64_t tile_total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)cnt, warp_tot, &tile_total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(d.lb_roots, tile, epoch, tile_total, &d.ctr->err);
+        if (threadIdx.x == 0) {
+            s_excl = ex;
+            if (tile == ntiles - 1) d.ctr->n_roots = (uint32_t)(ex + tile_total);
+        }
+    }
+    __syncthreads();
+    uint32_t pos = (uint32_t)(s_excl + incl - cnt);
+#pragma unroll
+    for (int q = 0; q < kRootWords; ++q) {
+        uint32_t bits = words[q];
+        while (bits) {
+            roots[pos++] = ((w0 + q) << 5) + (uint32_t)(__ffs(bits) - 1);
+            bits &= bits - 1u;
+        }
     }
 }
 
@@ -656,16 +712,14 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
 // dense labels in root order, dropped ones smallest - index - 1.
 
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t* roots0, const uint32_t* roots1,
-                                                    ClusterTables t, ClusterTables nt) {
+__global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t* roots, ClusterTables t,
+                                                    ClusterTables nt) {
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_roots;
     const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
     const uint32_t tile = fetch_tile(d.ctr, kSiteRelabel);
     if (tile >= ntiles) return;
-    const uint32_t sel = sorted_sel(d.sort);
-    const uint32_t* roots = sel ? roots1 : roots0;
     const uint32_t epoch = d.lb_epoch[kSiteRelabel];
     const int e = fixed_exponent(d.ctr->xmax_walk_bits, d.nb_bits);
     const double inv = pow2(-e);
@@ -1084,19 +1138,12 @@ __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
         const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;   // cut labels are c or K + c
         if (c >= k || !d.split[c]) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
+        uint32_t hint = ld_relaxed(&d.parent[v]);
         for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge || nb >= v || d.lab[nb] != lv) continue;
-            uint32_t a = v, b = nb;
-            for (uint32_t tries = 0;; ++tries) {
-                if (tries > kSpinLimit) { atomicOr(&d.ctr->err, kErrUnionFind); break; }
-                const uint32_t ra = uf_find(d.parent, a), rb = uf_find(d.parent, b);
-                if (ra == rb) break;
-                const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
-                if (atomicCAS(&d.parent[hi], hi, lo) == hi) break;
-                a = hi;
-                b = lo;
-            }
+            if (nb == kInvalidEdge) continue;
+            if (nb >= v) break;
+            if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
     }
 }

@@ -86,15 +86,18 @@ struct Dev {
     uint32_t* cut_off;
     uint8_t* split;
     void* allcuts;        // pxr_sweep_cut[]
-    // roots after the components stage
+    // roots after the components stage: a bitmap over vertex ids (zero
+    // between rounds), compacted into roots[0] in id order
     uint32_t* roots[2];
+    uint32_t* rootmap;
+    uint32_t n_words;
+    LookbackState lb_roots;
     // look-back state
     LookbackState lb_scan, lb_relabel, lb_apply, lb_ids, lb_cvol;
     uint32_t* lb_epoch;   // [8] current epoch per look-back site
     RoundCtr* ctr;
     SortState sort;
     uint32_t* sort_end_bit;   // main sort bits
-    uint32_t* root_end_bit;   // root sort bits
     uint32_t light_max;       // rows up to this many slots: W lanes per row in the round kernels
     const uint32_t* wide;     // vertices with light_max < row <= wide_max slots (one warp each)
     uint32_t n_wide;
@@ -130,7 +133,7 @@ constexpr uint32_t kChunkCapRows = 4096;
 // look-back sites (index into Dev::lb_epoch and RoundCtr::tile_counter)
 enum : int {
     kSiteScan = 0, kSiteRelabel = 1, kSiteApply = 2, kSiteIds = 3, kSiteCvol = 4,
-    kSiteFinal = 5, kSiteSched = 6, kSiteEmit = 7, kSiteCarry = 8
+    kSiteFinal = 5, kSiteSched = 6, kSiteEmit = 7, kSiteCarry = 8, kSiteRoots = 9
 };
 
 __device__ __forceinline__ uint32_t bitlen(uint32_t v) { return v ? 32u - __clz(v) : 0u; }

@@ -177,26 +177,21 @@ __global__ void __launch_bounds__(kBlock) k_carry_all(Dev<OffT> d, ClusterTables
 // Carried clusters: register their roots for the relabelling with data that
 // keeps them (count = size, spread 2, sum 0).
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTables t, uint32_t* roots) {
+__global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTables t) {
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     for (uint32_t c0 = blockIdx.x * blockDim.x; c0 < k; c0 += gridDim.x * blockDim.x) {
         const uint32_t c = c0 + threadIdx.x;
         const bool carried = c < k && !(d.sflag[c] & 1u);
-        uint32_t r = 0;
         if (carried) {
-            r = t.root[c];
+            const uint32_t r = t.root[c];
             d.acc_cnt[r] = t.size[c];
             d.acc_max[r] = ordered_bits(1.0f);
             d.acc_min[r] = ordered_bits(-1.0f);
             d.acc_sum[r] = 0;
             d.rootc[r] = (kOriginCarried << 30) | c;
+            mark_root(d, r);
         }
-        const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, carried);
-        uint32_t slot = 0;
-        if ((threadIdx.x & 31u) == 0 && ballot) slot = atomicAdd(&d.ctr->n_roots, (uint32_t)__popc(ballot));
-        slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-        if (carried) roots[slot + __popc(ballot & lanemask_lt())] = r;
     }
 }
 

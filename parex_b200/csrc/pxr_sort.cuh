@@ -114,7 +114,7 @@ __device__ __forceinline__ uint64_t sort_status_word(uint32_t epoch, uint32_t fl
 
 template <typename K>
 #ifndef PXR_SORT_MIN_BLOCKS
-#define PXR_SORT_MIN_BLOCKS 1
+#define PXR_SORT_MIN_BLOCKS 2
 #endif
 __global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_kernel(SortBuffers<K> b, SortState s, int pass,
                                                                  uint32_t* err) {
@@ -182,23 +182,23 @@ __global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_k
         whist[w][d] = tile_cnt;
         tile_cnt += c;
     }
+    // a status word carries its own count, so relaxed accesses suffice (no fences)
     uint64_t* st = s.status + (size_t)tile * kRadix + d;
-    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> mine(*st);
-    mine.store(sort_status_word(epoch, 1u, tile_cnt), cuda::memory_order_release);
+    st_relaxed64(st, sort_status_word(epoch, 1u, tile_cnt));
     uint32_t excl = 0;
     for (int32_t t = (int32_t)tile - 1; t >= 0; --t) {
-        cuda::atomic_ref<uint64_t, cuda::thread_scope_device> other(s.status[(size_t)t * kRadix + d]);
-        uint64_t w = other.load(cuda::memory_order_acquire);
+        const uint64_t* other = s.status + (size_t)t * kRadix + d;
+        uint64_t w = ld_relaxed64(other);
         uint32_t spins = 0;
         while ((uint32_t)(w >> 34) != (epoch & 0x3FFFFFFFu) || ((w >> 32) & 3u) == 0u) {
             if (++spins > kSpinLimit) { atomicOr(err, kErrSortTiles); break; }
             __nanosleep(32);
-            w = other.load(cuda::memory_order_acquire);
+            w = ld_relaxed64(other);
         }
         excl += (uint32_t)w;
         if (((w >> 32) & 3u) == 2u) break;
     }
-    mine.store(sort_status_word(epoch, 2u, excl + tile_cnt), cuda::memory_order_release);
+    st_relaxed64(st, sort_status_word(epoch, 2u, excl + tile_cnt));
     gbase[d] = s.bases[pass * kRadix + d] + excl;
     uint64_t total;
     const uint64_t incl = block_inclusive<Add64>((uint64_t)tile_cnt, warp_tot, &total);

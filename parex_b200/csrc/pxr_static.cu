@@ -54,11 +54,14 @@ constexpr size_t kCtr = align256(kLbInc + 8ull * kRankTiles);
 constexpr size_t kCount = align256(kCtr + sizeof(RoundCtr));
 constexpr size_t kEndBit = kCount + 4;
 constexpr size_t kBytes = align256(kEndBit + 4);
-constexpr size_t kCtrlWords = (kBytes - kCtrl) / 4;
+// words cleared per call: the control region up to the item count and end
+// bit, which block 0 writes while the other blocks clear (so never cleared)
+constexpr size_t kCtrlWords = (kCount - kCtrl) / 4;
 
 static __device__ __align__(256) unsigned char g_scratch[kBytes];
 
-// Clear the control region, then load (label ^ sign bit, vertex) pairs.
+// Clear the control region, then load (label ^ sign bit, vertex) pairs and
+// set the item count and end bit (outside the cleared words).
 __global__ void k_static_setup(unsigned char* base, const int32_t* labels, uint32_t n) {
     uint32_t* ctrl = reinterpret_cast<uint32_t*>(base + kCtrl);
     uint32_t* keys = reinterpret_cast<uint32_t*>(base + kKeys0);
