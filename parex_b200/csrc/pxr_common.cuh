@@ -63,6 +63,8 @@ struct RoundCtr {
     unsigned long long stat_swept_items;     // sweep input vertices, summed over rounds
     unsigned long long stat_skipped;         // cluster-rounds whose sweep the schedule skipped
     unsigned long long stat_false_stops;     // skipped sweeps that would have cut (audit mode)
+    unsigned long long stat_gsort_slots;     // round slots whose global-sort branch ran (graph driver)
+    unsigned long long stat_chunk_slots;     // round slots whose chunked-sort branch ran (graph driver)
 };
 
 // ---------------------------------------------------------------------------

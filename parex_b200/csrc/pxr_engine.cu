@@ -238,6 +238,7 @@ struct pxr_handle {
     std::string err;
     int device = 0;
     cudaStream_t own_stream = nullptr;
+    cudaStream_t side_stream = nullptr;   // captures the bodies of IF nodes
     cudaStream_t stream = nullptr;
     bool initialized = false;
     bool off64 = false;
@@ -309,6 +310,8 @@ struct pxr_handle {
     cudaGraphExec_t graphs[8] = {};  // device-driven loop, one per parity combination
     cudaGraphConditionalHandle conds[8] = {};
     uint64_t body_launches[8] = {};  // kernels per replay of the loop body
+    bool sort_regions = false;       // set while capturing: the body holds the sort IF nodes
+    bool body_regions[8] = {};
     uint32_t last_rounds = 0;
     double last_ms = 0.0;
     uint64_t launches = 0;
@@ -486,6 +489,55 @@ void hold_for_profiling(pxr_handle* h) {
     if (h->profiling) k_hold<<<1, 1, 0, h->stream>>>(300000u);
 }
 
+#define PXR_TRY(call)                      \
+    do {                                   \
+        const cudaError_t e_ = (call);     \
+        if (e_ != cudaSuccess) return e_;  \
+    } while (0)
+
+// kernels of the global sort (histogram, plan, 8 digit passes)
+constexpr uint64_t kGsortLaunches = 2 + kMaxPasses;
+
+// The graph being captured on h->stream, or null outside capture.
+cudaGraph_t capture_graph(pxr_handle* h) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &g) != cudaSuccess) return nullptr;
+    return cs == cudaStreamCaptureStatusActive ? g : nullptr;
+}
+
+// Run body(stream) under an IF node of the graph being captured on h->stream;
+// `cond` is set on the device by an earlier kernel of the same graph.
+// Without a handle, body runs on h->stream (its kernels guard themselves).
+template <class F>
+cudaError_t if_region(pxr_handle* h, cudaGraphConditionalHandle cond, F&& body) {
+    if (!cond) return body(h->stream);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &g, &deps, &ndeps);
+    if (e != cudaSuccess) return e;
+    if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+    cudaGraphNodeParams params{};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = cond;
+    params.conditional.type = cudaGraphCondTypeIf;
+    params.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, g, deps, ndeps, &params);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamBeginCaptureToGraph(h->side_stream, params.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const cudaError_t eb = body(h->side_stream);
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(h->side_stream, &captured);
+    if (e == cudaSuccess) e = eb;
+    if (e != cudaSuccess) return e;
+    return cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
 template <typename OffT, int W>
 cudaError_t op_walk(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
@@ -508,7 +560,17 @@ cudaError_t op_sweep(pxr_handle* h) {
     cudaStream_t s = h->stream;
     const ClusterTables& t = h->tab[h->tcur];
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1); });
+    // graph driver, plain form: the global sort and the chunked sort become
+    // IF nodes, so a round launches only the sort it uses
+    cudaGraphConditionalHandle c_gsort = 0, c_chunk = 0;
+    if (!h->sched.mode) {
+        if (cudaGraph_t g = capture_graph(h)) {
+            PXR_TRY(cudaGraphConditionalHandleCreate(&c_gsort, g, 1u, cudaGraphCondAssignDefault));
+            PXR_TRY(cudaGraphConditionalHandleCreate(&c_chunk, g, 1u, cudaGraphCondAssignDefault));
+            h->sort_regions = true;
+        }
+    }
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1, c_gsort, c_chunk); });
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     if (h->sched.mode)
         phase(h, kPhSched, 2, [&] {
@@ -533,11 +595,16 @@ cudaError_t op_sweep(pxr_handle* h) {
     b.end_bit = h->sort_end_bit;
     b.capacity = h->n;
     cudaError_t e = cudaSuccess;
-    phase(h, kPhSort, 3 + kMaxPasses, [&] {
-        e = radix_sort<uint64_t>(b, h->sort, &h->ctr->err, s, 64);
-        // the chunked sort writes buffer 0, which the idle global sort leaves selected
-        k_chunk_sort<OffT><<<std::min(std::max((h->n + kChunk - 1) / kChunk, 1u), 148u), kChunkThreads, chunk_sort_smem(), s>>>(
-            d, t, h->act[h->acur], h->par[h->acur], h->keys[0], h->vals[0]);
+    phase(h, kPhSort, kGsortLaunches + 1, [&] {
+        e = if_region(h, c_gsort, [&](cudaStream_t st) { return radix_sort<uint64_t>(b, h->sort, &h->ctr->err, st, 64); });
+        // the chunked sort writes buffer 0, which round preparation selects
+        if (e == cudaSuccess)
+            e = if_region(h, c_chunk, [&](cudaStream_t st) {
+                k_chunk_sort<OffT><<<std::min(std::max((h->n + kChunk - 1) / kChunk, 1u), 148u), kChunkThreads,
+                                     chunk_sort_smem(), st>>>(d, t, h->act[h->acur], h->par[h->acur], h->keys[0],
+                                                              h->vals[0]);
+                return cudaGetLastError();
+            });
     });
     if (e != cudaSuccess) return e;
     phase(h, kPhScan, 1, [&] {
@@ -693,9 +760,11 @@ pxr_status build_loop_graph(pxr_handle* h, int key) {
     const bool prof = h->profiling;
     h->profiling = false;
     const uint64_t launches_before = h->launches;
+    h->sort_regions = false;
     e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     cudaError_t e2 = e == cudaSuccess ? dispatch(h, kOpLoopBody, cond) : e;
     h->body_launches[key] = h->launches - launches_before;
+    h->body_regions[key] = h->sort_regions;
     h->launches = launches_before;   // counted when the graph runs
     cudaGraph_t captured = nullptr;
     if (e == cudaSuccess) e = cudaStreamEndCapture(h->stream, &captured);
@@ -726,11 +795,19 @@ pxr_status decompose_graph(pxr_handle* h) {
     k_loop_begin<<<1, 1, 0, h->stream>>>(h->ctr, h->cfg.max_rounds);
     PXR_CUDA(h, cudaGetLastError());
     const uint32_t before = h->h_ctr->rounds;
+    const uint64_t g0 = h->h_ctr->stat_gsort_slots, c0 = h->h_ctr->stat_chunk_slots;
     PXR_CUDA(h, cudaGraphLaunch(h->graphs[key], h->stream));
     pxr_status st = sync_ctr(h);
-    // the body (two rounds) ran ceil(rounds / 2) times, at least once
+    // the body (two rounds) ran ceil(rounds / 2) times, at least once; of the
+    // two sort IF nodes of each round slot only one ran
     const uint32_t ran = h->h_ctr->rounds - before;
-    h->launches += 1 + h->body_launches[key] * std::max<uint64_t>(1, (ran + 1) / 2);
+    const uint64_t iters = std::max<uint64_t>(1, (ran + 1) / 2);
+    if (h->body_regions[key]) {
+        const uint64_t dg = h->h_ctr->stat_gsort_slots - g0, dc = h->h_ctr->stat_chunk_slots - c0;
+        h->launches += 1 + iters * (h->body_launches[key] - 2 * (kGsortLaunches + 1)) + dg * kGsortLaunches + dc;
+    } else {
+        h->launches += 1 + h->body_launches[key] * iters;
+    }
     return st;
 }
 
@@ -1181,6 +1258,7 @@ pxr_status pxr_create(const pxr_config* cfg, pxr_handle** out) {
     if (h->device < 0 || h->device >= count) { delete h; return PXR_INVALID_ARG; }
     if (cudaSetDevice(h->device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&h->h_ctr, sizeof(RoundCtr)) != cudaSuccess) {
         delete h;
         return PXR_CUDA_ERROR;
@@ -1208,6 +1286,7 @@ void pxr_destroy(pxr_handle* h) {
     for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
     if (h->h_ctr) cudaFreeHost(h->h_ctr);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (h->side_stream) cudaStreamDestroy(h->side_stream);
     delete h;
 }
 

@@ -140,8 +140,11 @@ __device__ __forceinline__ uint32_t stream_col(const uint32_t* p) { return __ldc
 // round bookkeeping
 
 // stage: 0 before the walk, 1 before the sweep, 2 before the cut
+// In the graph driver, the global sort and the chunked sort of stage 1 sit
+// under two IF nodes whose conditions (gsort, chunk) are set here.
 template <typename OffT>
-__global__ void k_round_prep(Dev<OffT> d, int stage) {
+__global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle gsort = 0,
+                             cudaGraphConditionalHandle chunk = 0) {
     RoundCtr* c = d.ctr;
     c->n_cut = 0;
     c->n_roots = 0;
@@ -168,6 +171,14 @@ __global__ void k_round_prep(Dev<OffT> d, int stage) {
         if (c->chunk_path) {   // the chunked sort reads and writes every item once
             c->stat_sort_items += c->n_sweep;
             c->stat_sort_passes += 1;
+        }
+        // the chunked sort leaves its output in buffer 0 (the global sort,
+        // when it runs with no items, selects buffer 0 as well)
+        if (c->chunk_path) d.sort.pass_info[kMaxPasses] = 0u;
+        if (gsort) {
+            cudaGraphSetConditional(gsort, c->chunk_path ? 0u : 1u);
+            cudaGraphSetConditional(chunk, c->chunk_path ? 1u : 0u);
+            if (c->chunk_path) c->stat_chunk_slots += 1; else c->stat_gsort_slots += 1;
         }
     }
     if (stage == 2) c->max_csize_next = 0;
