@@ -56,8 +56,18 @@ typedef struct {
     uint32_t division;       /* PXR_DIV_*                                                 */
     uint32_t driver;         /* PXR_DRIVER_*                                              */
     uint32_t tune;           /* PXR_TUNE_* (row plan: lanes per row and row bins)          */
-    uint32_t reserved[8];
+    uint32_t components;     /* PXR_COMPONENTS_* (union-find schedule of the cut stage)    */
+    uint32_t reserved[7];
 } pxr_config;
+
+/* Union-find schedule of the connected-components stage (no counterpart in
+ * the reference, which hooks every edge).  Both give the same components. */
+enum {
+    PXR_COMPONENTS_AUTO = 0,    /* sampled from mean degree 16 on, plain below (default)  */
+    PXR_COMPONENTS_PLAIN = 1,   /* first-neighbour links, then every edge once            */
+    PXR_COMPONENTS_SAMPLED = 2  /* first-neighbour links, one hashed neighbour per vertex,
+                                   then full rows only outside each label's largest set   */
+};
 
 /* How the row plan of a graph is chosen (no counterpart in the reference,
  * whose kernels use one warp per vertex for every row). */

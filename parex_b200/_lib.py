@@ -40,10 +40,12 @@ STATIC_SCRATCH_MAX_LABELS = 65536
 class Config(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("sc_threshold", C.c_float), ("rw_threshold", C.c_float),
                 ("max_rounds", C.c_uint32), ("device", C.c_int32), ("division", C.c_uint32),
-                ("driver", C.c_uint32), ("tune", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+                ("driver", C.c_uint32), ("tune", C.c_uint32), ("components", C.c_uint32),
+                ("reserved", C.c_uint32 * 7)]
 
 
 TUNE_AUTO, TUNE_HEURISTIC = 0, 1
+COMPONENTS_AUTO, COMPONENTS_PLAIN, COMPONENTS_SAMPLED = 0, 1, 2
 
 
 class RowPlan(C.Structure):

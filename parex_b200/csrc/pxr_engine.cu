@@ -22,6 +22,7 @@ constexpr uint32_t kMaxGrid = 148u * 32u;
 #define PXR_UNION_LANES 1
 #endif
 constexpr int kUnionLanes = PXR_UNION_LANES;   // lanes per light row in k_union
+constexpr uint32_t kSampledDegree = 16;        // mean degree from which k_union uses sampled linking
 
 // ---------------------------------------------------------------------------
 // final partition on the device (PartitionManager::finalizePartition,
@@ -272,6 +273,7 @@ struct pxr_handle {
     uint32_t* cut_off = nullptr;
     uint8_t* split = nullptr;
     pxr_sweep_cut* allcuts = nullptr;
+    uint32_t* rep[2] = {nullptr, nullptr};
     uint32_t* roots[2] = {nullptr, nullptr};
     LookbackState lb[kSiteRoots + 1]{};
     uint32_t* rootmap = nullptr;
@@ -392,6 +394,13 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.pdif = h->pdif;
     d.pvol = h->pvol;
     d.cut_off = h->cut_off;
+    d.rep[0] = h->rep[0];
+    d.rep[1] = h->rep[1];
+    // sampled linking pays where rows are long (measured: 16k planted
+    // partition and 3D grids slower with it, 512-instance batch faster)
+    d.union_sampled = h->cfg.components == PXR_COMPONENTS_SAMPLED ? 1u
+                      : h->cfg.components == PXR_COMPONENTS_PLAIN ? 0u
+                      : (h->slots >= (uint64_t)kSampledDegree * h->n ? 1u : 0u);
     d.split = h->split;
     d.allcuts = h->allcuts;
     d.roots[0] = h->roots[0];
@@ -595,10 +604,21 @@ cudaError_t op_sweep(pxr_handle* h) {
     b.end_bit = h->sort_end_bit;
     b.capacity = h->n;
     cudaError_t e = cudaSuccess;
-    phase(h, kPhSort, kGsortLaunches + 1, [&] {
-        e = if_region(h, c_gsort, [&](cudaStream_t st) { return radix_sort<uint64_t>(b, h->sort, &h->ctr->err, st, 64); });
+    // per-phase timing (stream driver): read the round's choice and launch
+    // only that sort, as the graph driver's IF nodes do
+    bool run_gsort = true, run_chunk = true;
+    if (h->profiling && !c_gsort) {
+        uint32_t chunk_path = 0;
+        PXR_TRY(cudaMemcpyAsync(&chunk_path, &h->ctr->chunk_path, 4, cudaMemcpyDeviceToHost, s));
+        PXR_TRY(cudaStreamSynchronize(s));
+        run_gsort = chunk_path == 0;
+        run_chunk = chunk_path != 0;
+    }
+    phase(h, kPhSort, (run_gsort ? kGsortLaunches : 0) + (run_chunk ? 1 : 0), [&] {
+        if (run_gsort)
+            e = if_region(h, c_gsort, [&](cudaStream_t st) { return radix_sort<uint64_t>(b, h->sort, &h->ctr->err, st, 64); });
         // the chunked sort writes buffer 0, which round preparation selects
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && run_chunk)
             e = if_region(h, c_chunk, [&](cudaStream_t st) {
                 k_chunk_sort<OffT><<<std::min(std::max((h->n + kChunk - 1) / kChunk, 1u), 148u), kChunkThreads,
                                      chunk_sort_smem(), st>>>(d, t, h->act[h->acur], h->par[h->acur], h->keys[0],
@@ -633,9 +653,14 @@ cudaError_t op_cut(pxr_handle* h) {
     phase(h, kPhCutInit, 1, [&] {
         k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });
-    phase(h, kPhUnion, 3 + long_launches(h), [&] {
+    phase(h, kPhUnion, 3 + (d.union_sampled ? 3 : 0) + long_launches(h), [&] {
         k_link_first<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
         k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        if (d.union_sampled) {
+            k_union_sample<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
+            k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
+            k_union_reps<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1]);
+        }
         k_union<OffT, kUnionLanes><<<grid_for((uint64_t)h->n * kUnionLanes), kBlock, 0, s>>>(d, h->ids[h->acur]);
         PXR_LONG(h, k_union_long, d);
     });
@@ -651,7 +676,8 @@ cudaError_t op_cut(pxr_handle* h) {
         phase(h, kPhSched, 1, [&] {
             k_carry_vertices<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->act[h->acur], h->act[h->acur ^ 1]);
         });
-    phase(h, kPhApply, 1, [&] {
+    phase(h, kPhApply, 2, [&] {
+        k_newlab<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->ids[h->acur]);
         k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
                                                h->act[h->acur ^ 1], h->par[h->acur ^ 1]);
     });
@@ -871,7 +897,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     }
     A(&h->sflag, N); A(&h->nflag, N); A(&h->rootc, N); A(&h->mlp, (size_t)kMlpImage);
     if (h->sched.trace) { A(&h->records, N); }
-    A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N);
+    A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N); A(&h->rep[0], N); A(&h->rep[1], N);
     for (int i = 0; i <= kSiteRoots; ++i) {
         A(&h->lb[i].flags, scan_tiles); A(&h->lb[i].agg, scan_tiles); A(&h->lb[i].inc, scan_tiles);
     }
@@ -1248,7 +1274,8 @@ pxr_status pxr_create(const pxr_config* cfg, pxr_handle** out) {
     pxr_handle* h = new (std::nothrow) pxr_handle();
     if (!h) return PXR_OUT_OF_MEMORY;
     if (cfg) h->cfg = *cfg; else pxr_config_default(&h->cfg);
-    if (h->cfg.division > PXR_DIV_REFERENCE || h->cfg.driver > PXR_DRIVER_STREAM) {
+    if (h->cfg.division > PXR_DIV_REFERENCE || h->cfg.driver > PXR_DRIVER_STREAM ||
+        h->cfg.components > PXR_COMPONENTS_SAMPLED) {
         delete h;
         return PXR_INVALID_ARG;
     }

@@ -581,9 +581,69 @@ __device__ __forceinline__ void uf_join(uint32_t* parent, uint32_t* err, uint32_
     }
 }
 
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7FEB352Du; x ^= x >> 15; x *= 0x846CA68Bu; x ^= x >> 16;
+    return x;
+}
+
+// Sampled linking: each vertex of a split cluster joins one more same-label
+// neighbour, picked by a hash of its id.  With the first-link forest this
+// usually leaves one large set per label.
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_union_sample(Dev<OffT> d, const uint32_t* ids) {
+    if (d.ctr->walk_only) return;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        const uint32_t v = ids[j];
+        const int32_t lv = d.lab[v];
+        if (!in_split(d, k, lv)) continue;
+        const OffT beg = d.off[v], end = d.off[v + 1];
+        if (end == beg) continue;
+        const uint32_t nb = d.cols[beg + (OffT)(mix32(v) % (uint64_t)(end - beg))];
+        if (nb == kInvalidEdge || d.lab[nb] != lv) continue;
+        uint32_t hint = ld_relaxed(&d.parent[v]);
+        uf_join(d.parent, &d.ctr->err, v, nb, hint);
+    }
+}
+
+// Representatives: per split cluster, the root of its first sorted vertex
+// (label c) and, when cut, of its last (label k + c).
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_union_reps(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
+                                                       const uint32_t* vals1) {
+    if (d.ctr->walk_only) return;
+    const uint32_t k = d.ctr->n_clusters;
+    const uint32_t* vals = d.ctr->main_sel ? vals1 : vals0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < k; c += gridDim.x * blockDim.x) {
+        if (!d.split[c]) continue;
+        const uint32_t st = t.start[c], sz = t.size[c];
+        d.rep[0][c] = uf_find(d.parent, vals[st]);
+        if (d.cut_off[c] != kNoCut && sz > 0) d.rep[1][c] = uf_find(d.parent, vals[st + sz - 1]);
+    }
+}
+
 // union over same-label valid edges (ConsolidationManager::consolidate,
 // cuda/devConsolidate.h:46-112, 168-204), each undirected edge once (from its
 // larger end; rows are sorted, so a lane stops at the first neighbour >= v).
+// With the sampled linking (d.union_sampled), a vertex whose set is its
+// label's representative set skips its row, and the others join every
+// same-label neighbour: an edge is then either joined from an end outside
+// that set or has both ends inside it.  Without it, every edge is joined
+// once, from its larger end.
+template <typename OffT>
+__device__ __forceinline__ bool union_skip_row(const Dev<OffT>& d, uint32_t k, uint32_t v, int32_t lv,
+                                               uint32_t& hint) {
+    if (!d.union_sampled) {
+        hint = ld_relaxed(&d.parent[v]);
+        return false;
+    }
+    const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;
+    const uint32_t rep = (uint32_t)lv >= k ? d.rep[1][c] : d.rep[0][c];
+    hint = uf_find(d.parent, v);
+    return hint == rep;
+}
+
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* ids) {
     if (d.ctr->walk_only) return;
@@ -597,11 +657,12 @@ __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* i
         if (!in_split(d, k, lv)) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
         if ((uint64_t)(end - beg) > d.light_max) continue;   // k_union_long
-        uint32_t hint = ld_relaxed(&d.parent[v]);
+        uint32_t hint;
+        if (union_skip_row(d, k, v, lv, hint)) continue;
         for (OffT s = beg + gl; s < end; s += W) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge) continue;
-            if (nb >= v) break;
+            if (nb == kInvalidEdge || nb == v) continue;
+            if (!d.union_sampled && nb > v) break;   // each edge once, from its larger end
             if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
     }
@@ -618,6 +679,8 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                             const uint32_t* vals1, const uint64_t* keys0,
                                                             const uint64_t* keys1) {
+    // the sorted order: a cluster's items are contiguous, so runs of one root
+    // are long and the per-root atomics few
     const uint32_t count = d.ctr->n_sweep;
     const uint32_t sel = d.ctr->main_sel;
     const uint32_t* vals = sel ? vals1 : vals0;
@@ -811,8 +874,28 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
     if ((threadIdx.x & 31u) == 0 && biggest) atomicMax(&d.ctr->max_csize_next, biggest);
 }
 
-// new labels, recentering (x -= cluster mean) and the stable compaction of
-// the sorted order into the next round's active list.
+// Plain form: new labels and recentering (x -= cluster mean) over the
+// active list in vertex order, so labels, parents and potentials are read
+// and written in runs (k_apply then only compacts the sorted order).
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_newlab(Dev<OffT> d, ClusterTables t, const uint32_t* ids) {
+    if (d.ctr->walk_only || d.sched) return;
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
+        const uint32_t v = ids[j];
+        const uint32_t lv = (uint32_t)d.lab[v];   // c, or k + c past a cut
+        const uint32_t c = lv >= k ? lv - k : lv;
+        // k_components_data left parent[v] at the root
+        const uint32_t r = d.split[c] ? d.parent[v] : t.root[c];
+        const int32_t nl = d.newlab[r];
+        d.lab[v] = nl;
+        if (nl >= 0) d.x[v] = __double2float_rn(__dsub_rn((double)d.x[v], d.avg[r]));
+    }
+}
+
+// new labels and recentering (learned schedule only), and the stable
+// compaction of the sorted order into the next round's active list.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                   const uint32_t* vals1, const uint64_t* keys0,
@@ -840,9 +923,13 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
         if (i >= count) continue;
         const uint32_t c = (uint32_t)(keys[i] >> 32);
         cc[k] = c;
-        if (d.sched && !(d.sflag[c] & 1u)) continue;   // carried: k_carry_vertices
         const uint32_t v = vals[i];
         vv[k] = v;
+        if (!d.sched) {   // k_newlab wrote the new labels in vertex order
+            if (d.lab[v] >= 0) { keepmask |= 1u << k; ++run; }
+            continue;
+        }
+        if (!(d.sflag[c] & 1u)) continue;   // carried: k_carry_vertices
         // k_components_data left parent[v] at the root (atomicMin stores only
         // ever move a pointer towards the root)
         const uint32_t r = d.split[c] ? d.parent[v] : t.root[c];
@@ -1149,11 +1236,12 @@ __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
         const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;   // cut labels are c or K + c
         if (c >= k || !d.split[c]) continue;
         const OffT beg = d.off[v], end = d.off[v + 1];
-        uint32_t hint = ld_relaxed(&d.parent[v]);
+        uint32_t hint;
+        if (union_skip_row(d, k, v, lv, hint)) continue;
         for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge) continue;
-            if (nb >= v) break;
+            if (nb == kInvalidEdge || nb == v) continue;
+            if (!d.union_sampled && nb > v) break;
             if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
     }

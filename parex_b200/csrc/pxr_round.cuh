@@ -84,6 +84,8 @@ struct Dev {
     uint32_t* pvol;
     // per cluster
     uint32_t* cut_off;
+    uint32_t* rep[2];     // per split cluster: root of its first / last sorted vertex (sampled union)
+    uint32_t union_sampled;   // components by sampled linking (graphs of mean degree >= kSampledDegree)
     uint8_t* split;
     void* allcuts;        // pxr_sweep_cut[]
     // roots after the components stage: a bitmap over vertex ids (zero

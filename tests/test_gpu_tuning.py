@@ -89,3 +89,23 @@ def test_forced_plan_validation_and_reset():
     dm.expanderDecomposition()
     dm.set_row_plan()
     assert dm.row_plan()["source"] in (1, 2)
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_components_schedules_agree(name):
+    """Plain and sampled union-find give the same components, so the same
+    decomposition, in both drivers (the sampled schedule skips the rows of
+    each label's representative set: a different order of joins only)."""
+    g = GRAPHS[name]()
+    out = []
+    for comp in (P.COMPONENTS_PLAIN, P.COMPONENTS_SAMPLED):
+        for driver in (P.DRIVER_GRAPH, P.DRIVER_STREAM):
+            dm = P.CudaDeviceManager(driver=driver, components=comp)
+            dm.initialize(g)
+            dm.expanderDecomposition()
+            out.append((dm.getFinalPartition().clusterIds, dm.getNumCutEdges(), dm.downloadLabels()))
+            dm.close()
+    for ids, cut, lab in out[1:]:
+        np.testing.assert_array_equal(ids, out[0][0])
+        assert cut == out[0][1]
+        np.testing.assert_array_equal(lab, out[0][2])
