@@ -24,6 +24,11 @@ constexpr uint32_t kSpinLimit = 1u << 20;
 // Look-back sites (dynamic tile counters and epochs), one per scan kernel.
 constexpr int kSites = 12;
 
+// The walk's traffic counters (vertices, slots, gathers) are spread over
+// this many slot triples (block b adds to slot b mod kStatSlots) so that
+// their atomics do not queue on one L2 address; the host sums the slots.
+constexpr uint32_t kStatSlots = 32;
+
 // Per-round scalars kept on the device so rounds need no host round trip.
 struct RoundCtr {
     uint32_t n_active;        // active vertices (sweep input size)
@@ -55,10 +60,7 @@ struct RoundCtr {
     uint32_t max_csize_next;  // largest cluster kept for the next round
     uint32_t walk_only;       // learned schedule: no cluster is due this round, only the walk runs
     uint32_t pad1;
-    unsigned long long stat_walk_vertices;  // traffic counters since initialisation
-    unsigned long long stat_walk_slots;
-    unsigned long long stat_walk_gathers;
-    unsigned long long stat_sort_items;
+    unsigned long long stat_sort_items;     // traffic counters since initialisation (the walk's: kStatSlots)
     unsigned long long stat_sort_passes;
     unsigned long long stat_swept_items;     // sweep input vertices, summed over rounds
     unsigned long long stat_skipped;         // cluster-rounds whose sweep the schedule skipped

@@ -273,6 +273,7 @@ struct pxr_handle {
     uint32_t* cut_off = nullptr;
     uint8_t* split = nullptr;
     pxr_sweep_cut* allcuts = nullptr;
+    unsigned long long* walk_stats = nullptr;
     uint32_t* rep[2] = {nullptr, nullptr};
     uint32_t* roots[2] = {nullptr, nullptr};
     LookbackState lb[kSiteRoots + 1]{};
@@ -394,6 +395,7 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.pdif = h->pdif;
     d.pvol = h->pvol;
     d.cut_off = h->cut_off;
+    d.walk_stats = h->walk_stats;
     d.rep[0] = h->rep[0];
     d.rep[1] = h->rep[1];
     // sampled linking pays where rows are long (measured: 16k planted
@@ -898,6 +900,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->sflag, N); A(&h->nflag, N); A(&h->rootc, N); A(&h->mlp, (size_t)kMlpImage);
     if (h->sched.trace) { A(&h->records, N); }
     A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N); A(&h->rep[0], N); A(&h->rep[1], N);
+    A(&h->walk_stats, 3 * kStatSlots);
     for (int i = 0; i <= kSiteRoots; ++i) {
         A(&h->lb[i].flags, scan_tiles); A(&h->lb[i].agg, scan_tiles); A(&h->lb[i].inc, scan_tiles);
     }
@@ -918,6 +921,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     cudaStream_t s = h->stream;
     for (int i = 0; i <= kSiteRoots; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->rootmap, 0, (N / 32 + 1) * 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->walk_stats, 0, 3 * kStatSlots * sizeof(unsigned long long), s));
     PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, kSites * 4, s));
     h->records_n = h->records ? (uint32_t)N : 0u;
     if (!h->mlp_img.empty())
@@ -1590,9 +1594,17 @@ pxr_status pxr_get_stats(pxr_handle* h, pxr_stats* out) {
     out->active_vertices = h->h_ctr->n_active;
     out->active_clusters = h->h_ctr->n_clusters;
     out->clusters_with_cut = h->h_ctr->n_cut;
-    out->walk_vertices = h->h_ctr->stat_walk_vertices;
-    out->walk_slots = h->h_ctr->stat_walk_slots;
-    out->walk_gathers = h->h_ctr->stat_walk_gathers;
+    unsigned long long ws[3 * kStatSlots] = {};
+    if (h->walk_stats) {
+        PXR_CUDA(h, cudaMemcpyAsync(ws, h->walk_stats, sizeof(ws), cudaMemcpyDeviceToHost, h->stream));
+        PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    out->walk_vertices = out->walk_slots = out->walk_gathers = 0;
+    for (uint32_t q = 0; q < kStatSlots; ++q) {
+        out->walk_vertices += ws[3 * q];
+        out->walk_slots += ws[3 * q + 1];
+        out->walk_gathers += ws[3 * q + 2];
+    }
     out->sort_items = h->h_ctr->stat_sort_items;
     out->sort_passes = h->h_ctr->stat_sort_passes;
     out->swept_items = h->h_ctr->stat_swept_items;

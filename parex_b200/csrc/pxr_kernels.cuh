@@ -220,6 +220,60 @@ __global__ void k_loop_cond(Dev<OffT> d, cudaGraphConditionalHandle cond) {
 // (fusedRandomWalk_WarpParallel, cuda/devRandomWalk.h:117-203), W lanes per
 // vertex, vertices in id order, exact fixed-point sum.
 
+// Block-wide max of v, then one atomicMax per block on `addr` (atomics from
+// every warp on one word queue behind each other at its L2 slice).  Every
+// thread of the block must call it.
+__device__ __forceinline__ void block_atomic_max(uint32_t* addr, uint32_t v) {
+    __shared__ uint32_t s_m[kBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    if ((threadIdx.x & 31u) == 0) s_m[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t q = 1; q < blockDim.x / 32; ++q) v = max(v, s_m[q]);
+        if (v) atomicMax(addr, v);
+    }
+    __syncthreads();
+}
+
+// The walk's max |x'| and traffic counters: summed per block, then one
+// atomic per counter and block, the counters spread over kStatSlots slots
+// (per-warp atomics on four words cost 3 of 27 ms on the 128^3 grid).
+template <typename OffT>
+__device__ __forceinline__ void walk_block_totals(const Dev<OffT>& d, uint32_t vmax, unsigned long long st_v,
+                                                  unsigned long long st_s, unsigned long long st_g) {
+    __shared__ uint32_t s_vmax[kBlock / 32];
+    __shared__ unsigned long long s_st[3][kBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+        st_v += __shfl_xor_sync(0xFFFFFFFFu, st_v, o);
+        st_s += __shfl_xor_sync(0xFFFFFFFFu, st_s, o);
+        st_g += __shfl_xor_sync(0xFFFFFFFFu, st_g, o);
+    }
+    const uint32_t w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31u) == 0) {
+        s_vmax[w] = vmax;
+        s_st[0][w] = st_v;
+        s_st[1][w] = st_s;
+        s_st[2][w] = st_g;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t q = 1; q < blockDim.x / 32; ++q) {
+            vmax = max(vmax, s_vmax[q]);
+            st_v += s_st[0][q];
+            st_s += s_st[1][q];
+            st_g += s_st[2][q];
+        }
+        if (vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
+        unsigned long long* slot = d.walk_stats + 3 * (blockIdx.x % kStatSlots);
+        if (st_v) atomicAdd(&slot[0], st_v);
+        if (st_s) atomicAdd(&slot[1], st_s);
+        if (st_g) atomicAdd(&slot[2], st_g);
+    }
+}
+
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* ids, const float* xt_in,
                                                  float* xt_out) {
@@ -266,21 +320,7 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
             vmax = b > vmax ? b : vmax;
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
-        st_v += __shfl_xor_sync(0xFFFFFFFFu, st_v, o);
-        st_s += __shfl_xor_sync(0xFFFFFFFFu, st_s, o);
-        st_g += __shfl_xor_sync(0xFFFFFFFFu, st_g, o);
-    }
-    if ((threadIdx.x & 31u) == 0) {
-        if (vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
-        if (st_v) {
-            atomicAdd(&d.ctr->stat_walk_vertices, st_v);
-            atomicAdd(&d.ctr->stat_walk_slots, st_s);
-            atomicAdd(&d.ctr->stat_walk_gathers, st_g);
-        }
-    }
+    walk_block_totals(d, vmax, st_v, st_s, st_g);
 }
 
 // ---------------------------------------------------------------------------
@@ -869,9 +909,7 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) most_negative = min(most_negative, __shfl_xor_sync(0xFFFFFFFFu, most_negative, o));
     if ((threadIdx.x & 31u) == 0 && most_negative < 0) atomicMin(&d.ctr->smallest_next, most_negative);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) biggest = max(biggest, __shfl_xor_sync(0xFFFFFFFFu, biggest, o));
-    if ((threadIdx.x & 31u) == 0 && biggest) atomicMax(&d.ctr->max_csize_next, biggest);
+    block_atomic_max(&d.ctr->max_csize_next, biggest);
 }
 
 // Plain form: new labels and recentering (x -= cluster mean) over the
@@ -1064,10 +1102,7 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
             }
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
-    if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(&d.ctr->xmax_bits, vmax);
-    __syncthreads();
+    block_atomic_max(&d.ctr->xmax_bits, vmax);
     for (uint32_t q = threadIdx.x; q < kScanTile; q += kBlock)
         if (s_hkey[q] != 0xFFFFFFFFu && s_hval[q]) atomicAdd(&nt.vol[s_hkey[q]], s_hval[q]);
 }
@@ -1171,21 +1206,7 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
             st_s += (unsigned long long)(end - beg);
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
-        st_v += __shfl_xor_sync(0xFFFFFFFFu, st_v, o);
-        st_s += __shfl_xor_sync(0xFFFFFFFFu, st_s, o);
-        st_g += __shfl_xor_sync(0xFFFFFFFFu, st_g, o);
-    }
-    if ((threadIdx.x & 31u) == 0) {
-        if (vmax) atomicMax(&d.ctr->xmax_walk_bits, vmax);
-        if (st_v) {
-            atomicAdd(&d.ctr->stat_walk_vertices, st_v);
-            atomicAdd(&d.ctr->stat_walk_slots, st_s);
-        }
-        if (st_g) atomicAdd(&d.ctr->stat_walk_gathers, st_g);
-    }
+    walk_block_totals(d, vmax, st_v, st_s, st_g);
 }
 
 template <typename OffT, int G>

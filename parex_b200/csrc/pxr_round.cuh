@@ -85,6 +85,7 @@ struct Dev {
     // per cluster
     uint32_t* cut_off;
     uint32_t* rep[2];     // per split cluster: root of its first / last sorted vertex (sampled union)
+    unsigned long long* walk_stats;   // [kStatSlots][3]: walk vertices, slots, gathers
     uint32_t union_sampled;   // components by sampled linking (graphs of mean degree >= kSampledDegree)
     uint8_t* split;
     void* allcuts;        // pxr_sweep_cut[]
