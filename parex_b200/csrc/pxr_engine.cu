@@ -673,7 +673,8 @@ cudaError_t op_cut(pxr_handle* h) {
     // roots in vertex-id order (the order of the reference's root sort)
     const uint32_t root_tiles = (uint32_t)(((h->n + 31u) / 32u + kRootTileWords - 1) / kRootTileWords);
     phase(h, kPhRootSort, 1, [&] { k_root_compact<OffT><<<std::max(root_tiles, 1u), kBlock, 0, s>>>(d, h->roots[0]); });
-    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<tiles, kBlock, 0, s>>>(d, h->roots[0], t, nt); });
+    const uint32_t relabel_tiles = std::min(std::max((h->n + kRelabelTile - 1) / kRelabelTile, 1u), 148u * 8u);
+    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<relabel_tiles, kBlock, 0, s>>>(d, h->roots[0], t, nt); });
     if (h->sched.mode)
         phase(h, kPhSched, 1, [&] {
             k_carry_vertices<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->act[h->acur], h->act[h->acur ^ 1]);
@@ -883,7 +884,8 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     h->slots = 2 * m;
     h->off64 = sizeof(OffT) == 8;
     const size_t N = std::max<uint32_t>(n, 1);
-    const uint32_t scan_tiles = (uint32_t)((N + kScanTile - 1) / kScanTile) + 1;
+    // look-back state per site, sized for the smallest tile (k_relabel's)
+    const uint32_t scan_tiles = (uint32_t)((N + kRelabelTile - 1) / kRelabelTile) + 1;
     const uint32_t sort_tiles = (uint32_t)((N + kSortTile - 1) / kSortTile) + 1;
     cudaError_t e = cudaSuccess;
 #define A(ptr, cnt) if (e == cudaSuccess) e = dalloc(h, ptr, cnt)

@@ -11,6 +11,10 @@ namespace pxr {
 constexpr int kBlock = 256;
 constexpr int kScanItems = 8;                        // items per thread in look-back kernels
 constexpr int kScanTile = kBlock * kScanItems;
+// k_relabel runs over the roots, often far fewer than the vertices: smaller
+// tiles keep more of its latency-bound gathers in flight
+constexpr int kRelabelItems = 2;
+constexpr int kRelabelTile = kBlock * kRelabelItems;
 
 // ---------------------------------------------------------------------------
 // Run aggregation: a thread holds the aggregates of the runs of equal keys in
@@ -831,80 +835,84 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_roots;
-    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
-    const uint32_t tile = fetch_tile(d.ctr, kSiteRelabel);
-    if (tile >= ntiles) return;
+    const uint32_t ntiles = (count + kRelabelTile - 1) / kRelabelTile;
     const uint32_t epoch = d.lb_epoch[kSiteRelabel];
     const int e = fixed_exponent(d.ctr->xmax_walk_bits, d.nb_bits);
     const double inv = pow2(-e);
     const int32_t smallest = d.ctr->smallest;
-    const uint32_t first = tile * kScanTile + threadIdx.x * kScanItems;
-    uint64_t vals[kScanItems];
-    uint64_t run = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t j = first + k;
-        uint64_t v = 0;
-        if (j < count) {
-            const uint32_t r = roots[j];
-            const uint32_t cnt = d.acc_cnt[r];
-            const float pot = __fsub_rn(from_ordered_bits(d.acc_max[r]), from_ordered_bits(d.acc_min[r]));
-            const bool keep = pot >= d.rw_threshold && cnt >= 2;
-            v = keep ? (((uint64_t)cnt << 32) | 1u) : 0ull;
-        }
-        vals[k] = v;
-        run = PairAdd::combine(run, v);
-    }
-    uint64_t tile_total;
-    const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
-    if (threadIdx.x < 32) {
-        const uint64_t ex = lookback_tile<PairAdd>(d.lb_relabel, tile, epoch, tile_total, &d.ctr->err);
-        if (threadIdx.x == 0) s_excl = ex;
-        if (threadIdx.x == 0 && tile == ntiles - 1) {
-            const uint64_t all = PairAdd::combine(ex, tile_total);
-            d.ctr->n_keep = (uint32_t)all;
-            d.ctr->n_active_next = (uint32_t)(all >> 32);
-        }
-    }
-    __syncthreads();
-    const uint32_t lo = (uint32_t)incl - (uint32_t)run;
-    const uint32_t hi = (uint32_t)(incl >> 32) - (uint32_t)(run >> 32);
-    uint64_t p = PairAdd::combine(s_excl, ((uint64_t)hi << 32) | lo);
     int32_t most_negative = 0;
     uint32_t biggest = 0;
+    // tiles in the order they are taken (look-back), several per block
+    for (;;) {
+        const uint32_t tile = fetch_tile(d.ctr, kSiteRelabel);
+        if (tile >= ntiles) break;
+        const uint32_t first = tile * kRelabelTile + threadIdx.x * kRelabelItems;
+        uint64_t vals[kRelabelItems];
+        uint64_t run = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t j = first + k;
-        if (j >= count) break;
-        const uint32_t r = roots[j];
-        if (vals[k]) {
-            const uint32_t nl = (uint32_t)p;
-            const uint32_t cnt = (uint32_t)(vals[k] >> 32);
-            biggest = cnt > biggest ? cnt : biggest;
-            d.newlab[r] = (int32_t)nl;
-            d.avg[r] = __ddiv_rn(__dmul_rn(__ll2double_rn(d.acc_sum[r]), inv), (double)cnt);
-            nt.size[nl] = cnt;
-            nt.start[nl] = (uint32_t)(p >> 32);
-            nt.root[nl] = r;
-            nt.best[nl] = ~0ull;
-            // a cluster that was not split keeps its rows, degrees and volume:
-            // only the clusters born from a split rescan their rows
-            const uint32_t info = d.rootc[r];
-            const uint32_t kind = info >> 30;
-            const uint32_t c = info & kOriginLabelMask;
-            d.nflag[nl] = kind == kOriginCarried ? kRowsCarried : kind == kOriginSwept ? kRowsKept : kRowsScan;
-            nt.vol[nl] = kind == kOriginChild ? 0u : t.vol[c];
-            if (kind == kOriginCarried) {
-                const uint16_t sk = t.skip[c];
-                nt.skip[nl] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
-                nt.hist[nl] = t.hist[c];
+        for (int k = 0; k < kRelabelItems; ++k) {
+            const uint32_t j = first + k;
+            uint64_t v = 0;
+            if (j < count) {
+                const uint32_t r = roots[j];
+                const uint32_t cnt = d.acc_cnt[r];
+                const float pot = __fsub_rn(from_ordered_bits(d.acc_max[r]), from_ordered_bits(d.acc_min[r]));
+                const bool keep = pot >= d.rw_threshold && cnt >= 2;
+                v = keep ? (((uint64_t)cnt << 32) | 1u) : 0ull;
             }
-        } else {
-            const int32_t nl = (int32_t)((uint32_t)smallest - j - 1u);
-            d.newlab[r] = nl;
-            most_negative = nl < most_negative ? nl : most_negative;
+            vals[k] = v;
+            run = PairAdd::combine(run, v);
         }
-        p = PairAdd::combine(p, vals[k]);
+        uint64_t tile_total;
+        const uint64_t incl = block_inclusive<PairAdd>(run, warp_tot, &tile_total);
+        if (threadIdx.x < 32) {
+            const uint64_t ex = lookback_tile<PairAdd>(d.lb_relabel, tile, epoch, tile_total, &d.ctr->err);
+            if (threadIdx.x == 0) s_excl = ex;
+            if (threadIdx.x == 0 && tile == ntiles - 1) {
+                const uint64_t all = PairAdd::combine(ex, tile_total);
+                d.ctr->n_keep = (uint32_t)all;
+                d.ctr->n_active_next = (uint32_t)(all >> 32);
+            }
+        }
+        __syncthreads();
+        const uint32_t lo = (uint32_t)incl - (uint32_t)run;
+        const uint32_t hi = (uint32_t)(incl >> 32) - (uint32_t)(run >> 32);
+        uint64_t p = PairAdd::combine(s_excl, ((uint64_t)hi << 32) | lo);
+#pragma unroll
+        for (int k = 0; k < kRelabelItems; ++k) {
+            const uint32_t j = first + k;
+            if (j >= count) break;
+            const uint32_t r = roots[j];
+            if (vals[k]) {
+                const uint32_t nl = (uint32_t)p;
+                const uint32_t cnt = (uint32_t)(vals[k] >> 32);
+                biggest = cnt > biggest ? cnt : biggest;
+                d.newlab[r] = (int32_t)nl;
+                d.avg[r] = __ddiv_rn(__dmul_rn(__ll2double_rn(d.acc_sum[r]), inv), (double)cnt);
+                nt.size[nl] = cnt;
+                nt.start[nl] = (uint32_t)(p >> 32);
+                nt.root[nl] = r;
+                nt.best[nl] = ~0ull;
+                // a cluster that was not split keeps its rows, degrees and volume:
+                // only the clusters born from a split rescan their rows
+                const uint32_t info = d.rootc[r];
+                const uint32_t kind = info >> 30;
+                const uint32_t c = info & kOriginLabelMask;
+                d.nflag[nl] = kind == kOriginCarried ? kRowsCarried : kind == kOriginSwept ? kRowsKept : kRowsScan;
+                nt.vol[nl] = kind == kOriginChild ? 0u : t.vol[c];
+                if (kind == kOriginCarried) {
+                    const uint16_t sk = t.skip[c];
+                    nt.skip[nl] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+                    nt.hist[nl] = t.hist[c];
+                }
+            } else {
+                const int32_t nl = (int32_t)((uint32_t)smallest - j - 1u);
+                d.newlab[r] = nl;
+                most_negative = nl < most_negative ? nl : most_negative;
+            }
+            p = PairAdd::combine(p, vals[k]);
+        }
+        __syncthreads();   // s_excl and warp_tot are reused by the next tile
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) most_negative = min(most_negative, __shfl_xor_sync(0xFFFFFFFFu, most_negative, o));
