@@ -554,7 +554,7 @@ cudaError_t op_walk(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 0); });
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 32, 0, s>>>(d, 0); });
     phase(h, kPhWalk, 1 + long_launches(h), [&] {
         k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
                                                                           h->xt[h->xcur ^ 1]);
@@ -581,7 +581,7 @@ cudaError_t op_sweep(pxr_handle* h) {
             h->sort_regions = true;
         }
     }
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 1, c_gsort, c_chunk); });
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 32, 0, s>>>(d, 1, c_gsort, c_chunk); });
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     if (h->sched.mode)
         phase(h, kPhSched, 2, [&] {
@@ -645,7 +645,7 @@ cudaError_t op_cut(pxr_handle* h) {
     const ClusterTables& nt = h->tab[h->tcur ^ 1];
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 1, 0, s>>>(d, 2); });
+    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 32, 0, s>>>(d, 2); });
     if (h->sched.mode)
         phase(h, kPhSched, 2, [&] {
             k_carry_all<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, nt, h->act[h->acur], h->act[h->acur ^ 1],

@@ -150,6 +150,14 @@ template <typename OffT>
 __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle gsort = 0,
                              cudaGraphConditionalHandle chunk = 0) {
     RoundCtr* c = d.ctr;
+    // one warp: lane i resets look-back site i, lane 0 does the rest (the
+    // sites' dependent read-modify-writes in one thread took ~4 us)
+    const uint32_t lane = threadIdx.x;
+    if (lane < (uint32_t)kSites) {
+        c->tile_counter[lane] = 0;
+        d.lb_epoch[lane] += 1;
+    }
+    if (lane != 0) return;
     c->n_cut = 0;
     c->n_roots = 0;
     if (stage == 0) {
@@ -159,10 +167,6 @@ __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle 
     c->smallest_next = 0;
     c->n_keep = 0;
     c->n_active_next = 0;
-    for (int i = 0; i < kSites; ++i) {
-        c->tile_counter[i] = 0;
-        d.lb_epoch[i] += 1;
-    }
     if (stage == 1) {
         c->n_due_items = 0;
         if (d.sched) c->n_sweep = 0;   // set by k_due_scan
@@ -562,6 +566,14 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t v) {
     return v;
 }
 
+// Root of v, left in parent[v] (the atomic only where v's parent is not the root).
+__device__ __forceinline__ uint32_t uf_find_flat(uint32_t* parent, uint32_t v) {
+    const uint32_t p0 = ld_relaxed(&parent[v]);
+    const uint32_t r = p0 == v ? v : uf_find(parent, p0);
+    if (r != p0) atomicMin(&parent[v], r);
+    return r;
+}
+
 // The three linking kernels walk this round's active list in vertex order
 // (the walk's list), so rows, labels and parent words of neighbouring ids are
 // read together; the forest they build does not depend on the order.
@@ -604,8 +616,7 @@ __global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
         const uint32_t v = ids[j];
         if (!in_split(d, k, d.lab[v])) continue;
-        const uint32_t r = uf_find(d.parent, v);
-        atomicMin(&d.parent[v], r);
+        uf_find_flat(d.parent, v);
     }
 }
 
@@ -746,8 +757,7 @@ __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, Cluster
             const uint32_t v = vals[i];
             uint32_t r;
             if (d.split[c]) {
-                r = uf_find(d.parent, v);
-                atomicMin(&d.parent[v], r);
+                r = uf_find_flat(d.parent, v);
                 if (r == v) {
                     mark_root(d, r);
                     d.rootc[r] = (kOriginChild << 30) | c;
