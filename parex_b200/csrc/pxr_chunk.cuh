@@ -83,10 +83,15 @@ __device__ __forceinline__ void chunk_pass(const uint64_t* sk, const uint32_t* s
     for (int k = 0; k < kChunkIPT; ++k) {
         const bool valid = dg[k] < 0x100u;
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, dg[k]);
-        const uint32_t before = valid ? whist[warp][dg[k]] : 0u;
-        __syncwarp();
+        // the lowest lane of each digit reads and advances the warp's count
+        const uint32_t leader = (uint32_t)__ffs(peers) - 1u;
+        uint32_t before = 0;
+        if (valid && lane == leader) {
+            before = whist[warp][dg[k]];
+            whist[warp][dg[k]] = before + __popc(peers);
+        }
+        before = __shfl_sync(0xFFFFFFFFu, before, leader);
         rank[k] = before + __popc(peers & lt);
-        if (valid && (peers & lt) == 0u) whist[warp][dg[k]] = before + __popc(peers);
         __syncwarp();
     }
     __syncthreads();

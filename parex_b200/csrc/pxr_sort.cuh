@@ -165,10 +165,16 @@ __global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_k
         const bool valid = idx < count;
         const uint32_t d = valid ? ((uint32_t)(key[k] >> shift) & 0xFFu) : 0x100u;
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        const uint32_t before = valid ? whist[warp][d] : 0u;
-        __syncwarp();
+        // the lowest lane of each digit reads and advances the warp's count,
+        // the others take the old count from it
+        const uint32_t leader = (uint32_t)__ffs(peers) - 1u;
+        uint32_t before = 0;
+        if (valid && lane == leader) {
+            before = whist[warp][d];
+            whist[warp][d] = before + __popc(peers);
+        }
+        before = __shfl_sync(0xFFFFFFFFu, before, leader);
         rank[k] = before + __popc(peers & lt);
-        if (valid && (peers & lt) == 0u) whist[warp][d] = before + __popc(peers);
         __syncwarp();
     }
     __syncthreads();
