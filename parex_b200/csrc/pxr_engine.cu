@@ -1193,11 +1193,11 @@ template <typename OffT>
 pxr_status batch_setup(pxr_handle* h, uint32_t n_inst, const uint32_t* starts) {
     const uint32_t n = h->n;
     cudaStream_t s = h->stream;
-    uint32_t* d_starts = nullptr;
-    unsigned long long* d_vol = nullptr;
-    cudaError_t e = cudaMalloc(&d_starts, ((size_t)n_inst + 1) * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&d_vol, (size_t)n_inst * 8);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_starts, starts, ((size_t)n_inst + 1) * 4, cudaMemcpyHostToDevice, s);
+    // scratch in the sort key buffers, free until the first round (every
+    // instance holds a vertex, so n_inst + 1 <= 2n words and n_inst <= n)
+    uint32_t* d_starts = reinterpret_cast<uint32_t*>(h->keys[0]);
+    unsigned long long* d_vol = reinterpret_cast<unsigned long long*>(h->keys[1]);
+    cudaError_t e = cudaMemcpyAsync(d_starts, starts, ((size_t)n_inst + 1) * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_vol, 0, (size_t)n_inst * 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(&h->d_check[3], 0, 4, s);
     if (e == cudaSuccess) {
@@ -1211,8 +1211,6 @@ pxr_status batch_setup(pxr_handle* h, uint32_t n_inst, const uint32_t* starts) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(vol.data(), d_vol, (size_t)n_inst * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, &h->d_check[3], 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(d_starts);
-    cudaFree(d_vol);
     if (e != cudaSuccess) return cuda_fail(h, e, "batched set-up");
     if (bad) return fail(h, PXR_INVALID_ARG, "an edge joins two instances");
     std::vector<uint32_t> start(n_inst), size(n_inst), vol32(n_inst), vol_start(n_inst), root(n_inst);
