@@ -122,6 +122,12 @@ __device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
     cuda::atomic_ref<uint64_t, cuda::thread_scope_device> r(*const_cast<uint64_t*>(p));
     return r.load(cuda::memory_order_relaxed);
 }
+// Programmatic dependent launch: the round kernels are launched so that they
+// may be scheduled while their predecessor in the stream drains; each waits
+// here, before touching memory, until that predecessor has completed and its
+// writes are visible (a no-op when the launch has no programmatic dependency).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void st_relaxed64(uint64_t* p, uint64_t v) {
     cuda::atomic_ref<uint64_t, cuda::thread_scope_device> r(*p);
     r.store(v, cuda::memory_order_relaxed);

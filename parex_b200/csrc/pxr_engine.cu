@@ -492,9 +492,27 @@ uint32_t wide_grid(const pxr_handle* h) { return std::min((h->n_wide + kBlock / 
 uint32_t heavy_grid(const pxr_handle* h) { return std::min(h->n_heavy, 148u * 16u); }
 #define PXR_LONG(h, kern, ...)                                                                         \
     do {                                                                                               \
-        if ((h)->n_wide) kern<OffT, 32><<<wide_grid(h), kBlock, 0, s>>>(__VA_ARGS__);                 \
-        if ((h)->n_heavy) kern<OffT, kBlock><<<heavy_grid(h), kBlock, 0, s>>>(__VA_ARGS__);           \
+        if ((h)->n_wide) launch_pdl(kern<OffT, 32>, wide_grid(h), kBlock, 0, s, __VA_ARGS__);          \
+        if ((h)->n_heavy) launch_pdl(kern<OffT, kBlock>, heavy_grid(h), kBlock, 0, s, __VA_ARGS__);    \
     } while (0)
+
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while its predecessor in the stream drains, and waits in pdl_wait() before
+// it reads anything.  Launch errors surface through cudaGetLastError().
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 void hold_for_profiling(pxr_handle* h) {
     if (h->profiling) k_hold<<<1, 1, 0, h->stream>>>(300000u);
@@ -505,6 +523,8 @@ void hold_for_profiling(pxr_handle* h) {
         const cudaError_t e_ = (call);     \
         if (e_ != cudaSuccess) return e_;  \
     } while (0)
+
+constexpr cudaGraphConditionalHandle kNoCond = 0;   // round preparation outside the IF-node form
 
 // kernels of the global sort (histogram, plan, 8 digit passes)
 constexpr uint64_t kGsortLaunches = 2 + kMaxPasses;
@@ -554,13 +574,13 @@ cudaError_t op_walk(pxr_handle* h) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 32, 0, s>>>(d, 0); });
+    phase(h, kPhBook, 1, [&] { launch_pdl(k_round_prep<OffT>, 1, 32, 0, s, d, 0, kNoCond, kNoCond); });
     phase(h, kPhWalk, 1 + long_launches(h), [&] {
-        k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur],
+        launch_pdl(k_walk<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur], h->xt[h->xcur],
                                                                           h->xt[h->xcur ^ 1]);
         PXR_LONG(h, k_walk_long, d, h->xt[h->xcur], h->xt[h->xcur ^ 1]);
     });
-    phase(h, kPhBook, 1, [&] { k_after_walk<OffT><<<1, 1, 0, s>>>(d); });
+    phase(h, kPhBook, 1, [&] { launch_pdl(k_after_walk<OffT>, 1, 1, 0, s, d); });
     h->xcur ^= 1;
     return cudaGetLastError();
 }
@@ -581,22 +601,22 @@ cudaError_t op_sweep(pxr_handle* h) {
             h->sort_regions = true;
         }
     }
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 32, 0, s>>>(d, 1, c_gsort, c_chunk); });
+    phase(h, kPhBook, 1, [&] { launch_pdl(k_round_prep<OffT>, 1, 32, 0, s, d, 1, c_gsort, c_chunk); });
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     if (h->sched.mode)
         phase(h, kPhSched, 2, [&] {
-            k_due_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t);
-            k_walk_only_check<OffT><<<1, 1, 0, s>>>(d);
+            launch_pdl(k_due_scan<OffT>, tiles, kBlock, 0, s, d, t);
+            launch_pdl(k_walk_only_check<OffT>, 1, 1, 0, s, d);
         });
     phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
-        k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur]);
         PXR_LONG(h, k_nodediff_long, d);
     });
     phase(h, kPhEmit, 1, [&] {
         if (h->sched.mode)
-            k_emit_sched<OffT><<<tiles, kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+            launch_pdl(k_emit_sched<OffT>, tiles, kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
         else
-            k_emit<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
+            launch_pdl(k_emit<OffT>, grid_for(h->n), kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
     });
     SortBuffers<uint64_t> b{};
     b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
@@ -632,7 +652,7 @@ cudaError_t op_sweep(pxr_handle* h) {
     phase(h, kPhScan, 1, [&] {
         k_sweep_scan<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->keys[0], h->keys[1], h->vals[0], h->vals[1]);
     });
-    phase(h, kPhClusterCut, 1, [&] { k_cluster_cut<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t); });
+    phase(h, kPhClusterCut, 1, [&] { launch_pdl(k_cluster_cut<OffT>, grid_for(h->n), kBlock, 0, s, d, t); });
     h->sweep_tab = h->tcur;
     return cudaGetLastError();
 }
@@ -645,53 +665,53 @@ cudaError_t op_cut(pxr_handle* h) {
     const ClusterTables& nt = h->tab[h->tcur ^ 1];
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     hold_for_profiling(h);
-    phase(h, kPhBook, 1, [&] { k_round_prep<OffT><<<1, 32, 0, s>>>(d, 2); });
+    phase(h, kPhBook, 1, [&] { launch_pdl(k_round_prep<OffT>, 1, 32, 0, s, d, 2, kNoCond, kNoCond); });
     if (h->sched.mode)
         phase(h, kPhSched, 2, [&] {
-            k_carry_all<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, nt, h->act[h->acur], h->act[h->acur ^ 1],
+            launch_pdl(k_carry_all<OffT>, grid_for(h->n), kBlock, 0, s, d, t, nt, h->act[h->acur], h->act[h->acur ^ 1],
                                                                  h->ids[h->acur], h->ids[h->acur ^ 1]);
-            k_carry_roots<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t);
+            launch_pdl(k_carry_roots<OffT>, grid_for(h->n), kBlock, 0, s, d, t);
         });
     phase(h, kPhCutInit, 1, [&] {
-        k_cut_init<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
+        launch_pdl(k_cut_init<OffT>, grid_for(h->n), kBlock, 0, s, d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1]);
     });
     phase(h, kPhUnion, 3 + (d.union_sampled ? 3 : 0) + long_launches(h), [&] {
-        k_link_first<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
-        k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        launch_pdl(k_link_first<OffT>, grid_for(h->n), kBlock, 0, s, d, h->ids[h->acur]);
+        launch_pdl(k_compress<OffT>, grid_for(h->n), kBlock, 0, s, d, h->ids[h->acur]);
         if (d.union_sampled) {
-            k_union_sample<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
-            k_compress<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, h->ids[h->acur]);
-            k_union_reps<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1]);
+            launch_pdl(k_union_sample<OffT>, grid_for(h->n), kBlock, 0, s, d, h->ids[h->acur]);
+            launch_pdl(k_compress<OffT>, grid_for(h->n), kBlock, 0, s, d, h->ids[h->acur]);
+            launch_pdl(k_union_reps<OffT>, grid_for(h->n), kBlock, 0, s, d, t, h->vals[0], h->vals[1]);
         }
-        k_union<OffT, kUnionLanes><<<grid_for((uint64_t)h->n * kUnionLanes), kBlock, 0, s>>>(d, h->ids[h->acur]);
+        launch_pdl(k_union<OffT, kUnionLanes>, grid_for((uint64_t)h->n * kUnionLanes), kBlock, 0, s, d, h->ids[h->acur]);
         PXR_LONG(h, k_union_long, d);
     });
     phase(h, kPhComponents, 1, [&] {
-        k_components_data<OffT><<<std::min(tiles, kMaxGrid), kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1],
+        launch_pdl(k_components_data<OffT>, std::min(tiles, kMaxGrid), kBlock, 0, s, d, t, h->vals[0], h->vals[1],
                                                                               h->keys[0], h->keys[1]);
     });
     // roots in vertex-id order (the order of the reference's root sort)
     const uint32_t root_tiles = (uint32_t)(((h->n + 31u) / 32u + kRootTileWords - 1) / kRootTileWords);
-    phase(h, kPhRootSort, 1, [&] { k_root_compact<OffT><<<std::max(root_tiles, 1u), kBlock, 0, s>>>(d, h->roots[0]); });
+    phase(h, kPhRootSort, 1, [&] { launch_pdl(k_root_compact<OffT>, std::max(root_tiles, 1u), kBlock, 0, s, d, h->roots[0]); });
     const uint32_t relabel_tiles = std::min(std::max((h->n + kRelabelTile - 1) / kRelabelTile, 1u), 148u * 8u);
-    phase(h, kPhRelabel, 1, [&] { k_relabel<OffT><<<relabel_tiles, kBlock, 0, s>>>(d, h->roots[0], t, nt); });
+    phase(h, kPhRelabel, 1, [&] { launch_pdl(k_relabel<OffT>, relabel_tiles, kBlock, 0, s, d, h->roots[0], t, nt); });
     if (h->sched.mode)
         phase(h, kPhSched, 1, [&] {
-            k_carry_vertices<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->act[h->acur], h->act[h->acur ^ 1]);
+            launch_pdl(k_carry_vertices<OffT>, tiles, kBlock, 0, s, d, t, h->act[h->acur], h->act[h->acur ^ 1]);
         });
     phase(h, kPhApply, 2, [&] {
-        k_newlab<OffT><<<grid_for(h->n), kBlock, 0, s>>>(d, t, h->ids[h->acur]);
-        k_apply<OffT><<<tiles, kBlock, 0, s>>>(d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
+        launch_pdl(k_newlab<OffT>, grid_for(h->n), kBlock, 0, s, d, t, h->ids[h->acur]);
+        launch_pdl(k_apply<OffT>, tiles, kBlock, 0, s, d, t, h->vals[0], h->vals[1], h->keys[0], h->keys[1],
                                                h->act[h->acur ^ 1], h->par[h->acur ^ 1]);
     });
     phase(h, kPhDisable, 1 + long_launches(h), [&] {
-        k_ids_disable<OffT, W><<<tiles, kBlock, 0, s>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
+        launch_pdl(k_ids_disable<OffT, W>, tiles, kBlock, 0, s, d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
         PXR_LONG(h, k_disable_long, d, h->xt[h->xcur], nt);
     });
-    phase(h, kPhCvol, 1, [&] { k_cvol_scan<OffT><<<tiles, kBlock, 0, s>>>(d, nt); });
+    phase(h, kPhCvol, 1, [&] { launch_pdl(k_cvol_scan<OffT>, tiles, kBlock, 0, s, d, nt); });
     if (h->sched.mode || d.trace)
-        phase(h, kPhSched, 1, [&] { k_schedule<OffT><<<std::min(grid_for(h->n), 148u * 8u), kBlock, 0, s>>>(d, t, nt); });
-    phase(h, kPhBook, 1, [&] { k_round_end<OffT><<<1, 1, 0, s>>>(d); });
+        phase(h, kPhSched, 1, [&] { launch_pdl(k_schedule<OffT>, std::min(grid_for(h->n), 148u * 8u), kBlock, 0, s, d, t, nt); });
+    phase(h, kPhBook, 1, [&] { launch_pdl(k_round_end<OffT>, 1, 1, 0, s, d); });
     h->tcur ^= 1;
     h->acur ^= 1;
     return cudaGetLastError();
@@ -712,7 +732,7 @@ cudaError_t op_loop_body(pxr_handle* h, cudaGraphConditionalHandle cond) {
     if (e == cudaSuccess) e = op_round<OffT, W>(h);
     if (e != cudaSuccess) return e;
     Dev<OffT> d = make_dev<OffT>(h);
-    phase(h, kPhBook, 1, [&] { k_loop_cond<OffT><<<1, 1, 0, h->stream>>>(d, cond); });
+    phase(h, kPhBook, 1, [&] { launch_pdl(k_loop_cond<OffT>, 1, 1, 0, h->stream, d, cond); });
     return cudaGetLastError();
 }
 

@@ -149,6 +149,7 @@ __device__ __forceinline__ uint32_t stream_col(const uint32_t* p) { return __ldc
 template <typename OffT>
 __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle gsort = 0,
                              cudaGraphConditionalHandle chunk = 0) {
+    pdl_wait();
     RoundCtr* c = d.ctr;
     // one warp: lane i resets look-back site i, lane 0 does the rest (the
     // sites' dependent read-modify-writes in one thread took ~4 us)
@@ -195,10 +196,14 @@ __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle 
 }
 
 template <typename OffT>
-__global__ void k_after_walk(Dev<OffT> d) { d.ctr->xmax_bits = d.ctr->xmax_walk_bits; }
+__global__ void k_after_walk(Dev<OffT> d) {
+    pdl_wait();
+    d.ctr->xmax_bits = d.ctr->xmax_walk_bits;
+}
 
 template <typename OffT>
 __global__ void k_round_end(Dev<OffT> d) {
+    pdl_wait();
     RoundCtr* c = d.ctr;
     if (c->n_active > 0) {
         c->rounds += 1;
@@ -218,6 +223,7 @@ __global__ void k_round_end(Dev<OffT> d) {
 // device-driven round loop: keep looping while clusters remain and the cap allows
 template <typename OffT>
 __global__ void k_loop_cond(Dev<OffT> d, cudaGraphConditionalHandle cond) {
+    pdl_wait();
     const RoundCtr* c = d.ctr;
     const bool more = !c->done && c->err == 0 && (c->rounds - c->loop_start) < c->loop_cap;
     cudaGraphSetConditional(cond, more ? 1u : 0u);
@@ -285,6 +291,7 @@ __device__ __forceinline__ void walk_block_totals(const Dev<OffT>& d, uint32_t v
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* ids, const float* xt_in,
                                                  float* xt_out) {
+    pdl_wait();
     const uint32_t count = d.ctr->n_active;
     const int e = fixed_exponent(d.ctr->xmax_bits, d.nb_bits);
     const double scale = pow2(e), inv = pow2(-e);
@@ -337,6 +344,7 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
 
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t* ids) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t count = d.ctr->n_active;
     const uint32_t gl = threadIdx.x & (W - 1);
@@ -378,6 +386,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_emit(Dev<OffT> d, const uint32_t* act, uint64_t* keys,
                                                  uint32_t* vals, uint64_t* best) {
+    pdl_wait();
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
     const bool emit = !d.ctr->chunk_path;   // the chunk path reads the active list itself
@@ -405,6 +414,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_sweep_scan(Dev<OffT> d, ClusterTables t, const uint64_t* keys0,
                                                        const uint64_t* keys1, const uint32_t* vals0,
                                                        const uint32_t* vals1) {
+    pdl_wait();
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_sweep;
@@ -487,6 +497,7 @@ __global__ void __launch_bounds__(kBlock) k_sweep_scan(Dev<OffT> d, ClusterTable
 // cuda/devSweepCut.h:321-331, 701-709) and the components plan.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTables t) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t full = d.ctr->full_components;
@@ -528,6 +539,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cut_init(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                      const uint32_t* vals1, const uint64_t* keys0,
                                                      const uint64_t* keys1) {
+    pdl_wait();
     const uint32_t count = d.ctr->n_sweep;
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t sel = d.ctr->main_sel;
@@ -584,6 +596,7 @@ __device__ __forceinline__ uint32_t uf_find_flat(uint32_t* parent, uint32_t v) {
 // accumulators for the component data start from the identity.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32_t* ids) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
@@ -610,6 +623,7 @@ __global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32
 // Flatten the linked forest: every vertex of a split cluster points at its root.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t* ids) {
+    pdl_wait();
     if (d.ctr->walk_only) return;
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
@@ -646,6 +660,7 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
 // usually leaves one large set per label.
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_union_sample(Dev<OffT> d, const uint32_t* ids) {
+    pdl_wait();
     if (d.ctr->walk_only) return;
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
@@ -667,6 +682,7 @@ __global__ void __launch_bounds__(kBlock) k_union_sample(Dev<OffT> d, const uint
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_union_reps(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                        const uint32_t* vals1) {
+    pdl_wait();
     if (d.ctr->walk_only) return;
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t* vals = d.ctr->main_sel ? vals1 : vals0;
@@ -701,6 +717,7 @@ __device__ __forceinline__ bool union_skip_row(const Dev<OffT>& d, uint32_t k, u
 
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* ids) {
+    pdl_wait();
     if (d.ctr->walk_only) return;
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
@@ -734,6 +751,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_components_data(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                             const uint32_t* vals1, const uint64_t* keys0,
                                                             const uint64_t* keys1) {
+    pdl_wait();
     // the sorted order: a cluster's items are contiguous, so runs of one root
     // are long and the per-root atomics few
     const uint32_t count = d.ctr->n_sweep;
@@ -795,6 +813,7 @@ constexpr uint32_t kRootTileWords = kBlock * kRootWords;
 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_root_compact(Dev<OffT> d, uint32_t* roots) {
+    pdl_wait();
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
@@ -842,6 +861,7 @@ __global__ void __launch_bounds__(kBlock) k_root_compact(Dev<OffT> d, uint32_t* 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t* roots, ClusterTables t,
                                                     ClusterTables nt) {
+    pdl_wait();
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_roots;
@@ -935,6 +955,7 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
 // and written in runs (k_apply then only compacts the sorted order).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_newlab(Dev<OffT> d, ClusterTables t, const uint32_t* ids) {
+    pdl_wait();
     if (d.ctr->walk_only || d.sched) return;
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
@@ -956,6 +977,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                   const uint32_t* vals1, const uint64_t* keys0,
                                                   const uint64_t* keys1, uint32_t* act_next, uint32_t* par_next) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
@@ -1019,6 +1041,7 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint32_t* ids, uint32_t* ids_next,
                                                         float* xt, ClusterTables nt) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
@@ -1184,6 +1207,7 @@ __device__ __forceinline__ const uint32_t* row_list(const Dev<OffT>& d, int G, u
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* xt_in, float* xt_out) {
+    pdl_wait();
     __shared__ int64_t sh[kBlock / 32];
     const int e = fixed_exponent(d.ctr->xmax_bits, d.nb_bits);
     const double scale = pow2(e), inv = pow2(-e);
@@ -1229,6 +1253,7 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ int32_t sh[kBlock / 32];
     uint32_t cnt;
@@ -1263,6 +1288,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     uint32_t cnt;
@@ -1288,6 +1314,7 @@ __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
 
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt, ClusterTables nt) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint32_t sh[kBlock / 32];
     uint32_t cnt;
@@ -1325,6 +1352,7 @@ __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt,
 // exclusive prefix of cluster volumes over labels
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_cvol_scan(Dev<OffT> d, ClusterTables nt) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;

@@ -23,6 +23,7 @@ namespace pxr {
 // per cluster: due / in-sweep flags and the start tables of the sweep set
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_due_scan(Dev<OffT> d, ClusterTables t) {
+    pdl_wait();
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
     const uint32_t count = d.ctr->n_clusters;
@@ -84,6 +85,7 @@ __global__ void __launch_bounds__(kBlock) k_due_scan(Dev<OffT> d, ClusterTables 
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_emit_sched(Dev<OffT> d, const uint32_t* act, uint64_t* keys,
                                                        uint32_t* vals, uint64_t* best) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
@@ -133,6 +135,7 @@ __global__ void __launch_bounds__(kBlock) k_emit_sched(Dev<OffT> d, const uint32
 // After the due scan: a round in which no cluster is due only walks.
 template <typename OffT>
 __global__ void k_walk_only_check(Dev<OffT> d) {
+    pdl_wait();
     d.ctr->walk_only = (d.ctr->n_sweep == 0 && d.ctr->n_active > 0) ? 1u : 0u;
 }
 
@@ -142,6 +145,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_carry_all(Dev<OffT> d, ClusterTables t, ClusterTables nt,
                                                       const uint32_t* act, uint32_t* act_next, const uint32_t* ids,
                                                       uint32_t* ids_next) {
+    pdl_wait();
     if (!d.ctr->walk_only) return;
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t na = d.ctr->n_active;
@@ -178,6 +182,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_all(Dev<OffT> d, ClusterTables
 // keeps them (count = size, spread 2, sum 0).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTables t) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     const uint32_t k = d.ctr->n_clusters;
     for (uint32_t c0 = blockIdx.x * blockDim.x; c0 < k; c0 += gridDim.x * blockDim.x) {
@@ -200,6 +205,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_roots(Dev<OffT> d, ClusterTabl
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_carry_vertices(Dev<OffT> d, ClusterTables t, const uint32_t* act,
                                                            uint32_t* act_next) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ uint64_t warp_tot[kBlock / 32];
     __shared__ uint64_t s_excl;
@@ -249,6 +255,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_vertices(Dev<OffT> d, ClusterT
 // were already handled by k_relabel (counter decremented, history kept).
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock, 1) k_schedule(Dev<OffT> d, ClusterTables t, ClusterTables nt) {
+    pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ float img[kMlpImage];
     if (d.sched)
