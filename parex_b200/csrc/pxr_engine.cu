@@ -570,7 +570,7 @@ cudaError_t if_region(pxr_handle* h, cudaGraphConditionalHandle cond, F&& body) 
 }
 
 template <typename OffT, int W>
-cudaError_t op_walk(pxr_handle* h) {
+cudaError_t op_walk(pxr_handle* h, bool in_round = false) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     hold_for_profiling(h);
@@ -580,7 +580,9 @@ cudaError_t op_walk(pxr_handle* h) {
                                                                           h->xt[h->xcur ^ 1]);
         PXR_LONG(h, k_walk_long, d, h->xt[h->xcur], h->xt[h->xcur ^ 1]);
     });
-    phase(h, kPhBook, 1, [&] { launch_pdl(k_after_walk<OffT>, 1, 1, 0, s, d); });
+    // the next walk's fixed-point scale follows max |x'|; inside a plain round
+    // the cut stage recomputes it over the recentred potentials anyway
+    if (!in_round || h->sched.mode) phase(h, kPhBook, 1, [&] { launch_pdl(k_after_walk<OffT>, 1, 1, 0, s, d); });
     h->xcur ^= 1;
     return cudaGetLastError();
 }
@@ -719,7 +721,7 @@ cudaError_t op_cut(pxr_handle* h) {
 
 template <typename OffT, int W>
 cudaError_t op_round(pxr_handle* h) {
-    cudaError_t e = op_walk<OffT, W>(h);
+    cudaError_t e = op_walk<OffT, W>(h, true);
     if (e == cudaSuccess) e = op_sweep<OffT, W>(h);
     if (e == cudaSuccess) e = op_cut<OffT, W>(h);
     return e;
