@@ -390,8 +390,9 @@ __global__ void __launch_bounds__(kBlock) k_emit(Dev<OffT> d, const uint32_t* ac
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
     const bool emit = !d.ctr->chunk_path;   // the chunk path reads the active list itself
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        if (emit) {
+    const uint32_t lim = emit ? max(count, k) : k;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += gridDim.x * blockDim.x) {
+        if (emit && i < count) {
             const uint32_t v = act[i];
             keys[i] = ((uint64_t)(uint32_t)d.lab[v] << 32) | ordered_bits(d.x[v]);
             vals[i] = v;
