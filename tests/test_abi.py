@@ -76,3 +76,15 @@ def test_create_fails_loudly_without_a_device():
     h = C.c_void_p()
     assert L.pxr_create(C.byref(cfg), C.byref(h)) == 4   # PXR_CUDA_ERROR: no CPU fallback
     assert not h.value
+
+
+def test_out_of_range_options_are_refused_before_any_device_work():
+    L = _lib.load()
+    for field, bad in (("division", 2), ("driver", 2), ("components", 3)):
+        cfg = _lib.Config()
+        L.pxr_config_default(C.byref(cfg))
+        assert cfg.components == _lib.COMPONENTS_AUTO
+        setattr(cfg, field, bad)
+        h = C.c_void_p()
+        assert L.pxr_create(C.byref(cfg), C.byref(h)) == 1, field   # PXR_INVALID_ARG
+        assert not h.value
