@@ -127,6 +127,10 @@ __device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
 // here, before touching memory, until that predecessor has completed and its
 // writes are visible (a no-op when the launch has no programmatic dependency).
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Let the next kernel in the stream be scheduled now (its blocks still wait
+// in pdl_wait for this kernel's completion); used by the one-block
+// bookkeeping kernels, which leave the rest of the GPU idle.
+__device__ __forceinline__ void pdl_launch_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ void st_relaxed64(uint64_t* p, uint64_t v) {
     cuda::atomic_ref<uint64_t, cuda::thread_scope_device> r(*p);

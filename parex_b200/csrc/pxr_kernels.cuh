@@ -150,6 +150,7 @@ template <typename OffT>
 __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle gsort = 0,
                              cudaGraphConditionalHandle chunk = 0) {
     pdl_wait();
+    pdl_launch_next();
     RoundCtr* c = d.ctr;
     // one warp: lane i resets look-back site i, lane 0 does the rest (the
     // sites' dependent read-modify-writes in one thread took ~4 us)
@@ -198,12 +199,14 @@ __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle 
 template <typename OffT>
 __global__ void k_after_walk(Dev<OffT> d) {
     pdl_wait();
+    pdl_launch_next();
     d.ctr->xmax_bits = d.ctr->xmax_walk_bits;
 }
 
 template <typename OffT>
 __global__ void k_round_end(Dev<OffT> d) {
     pdl_wait();
+    pdl_launch_next();
     RoundCtr* c = d.ctr;
     if (c->n_active > 0) {
         c->rounds += 1;
