@@ -114,3 +114,25 @@ def test_batched_rejects_malformed():
         dm.initialize_batched(joined, starts)
     dm.initialize_batched(g, starts)                          # still usable
     dm.expanderDecomposition()
+
+
+def test_batched_components_schedules_agree_with_the_oracle():
+    """The sampled union-find schedule on a batch with a one-vertex instance,
+    a one-edge instance and an instance of two disjoint triangles: the same
+    decomposition as the oracle's (representatives are per split cluster,
+    so instances never share one)."""
+    g, starts = _batch(count=10, seed=3, n_lo=10, n_hi=2000)
+    out = []
+    for comp in (P.COMPONENTS_PLAIN, P.COMPONENTS_SAMPLED):
+        dm = P.CudaDeviceManager(components=comp)
+        dm.initialize_batched(g, starts)
+        if not out:
+            orc, _ = _oracle_for(dm, g, starts)
+        dm.expanderDecomposition()
+        out.append((dm.getFinalPartition(), dm.getNumCutEdges()))
+    orc.decompose()
+    ids, k = orc.final_partition()
+    for fp, cut in out:
+        np.testing.assert_array_equal(fp.clusterIds, ids)
+        assert fp.numClusters == k
+        assert cut == orc.num_cut_edges()
