@@ -94,3 +94,44 @@ def test_device_sbm_batch_structure_and_decomposition():
     b.initialize_batched(g, starts)
     b.expanderDecomposition()
     np.testing.assert_array_equal(a.getFinalPartition().clusterIds, b.getFinalPartition().clusterIds)
+
+
+def test_device_batch_at_scale_size_independent_properties():
+    """A 64-instance device-built batch (about 10 M vertices, mean degree about
+    18, so the default components schedule is the sampled one): graph and
+    stream drivers and both union-find schedules give the same partition, and
+    the device cut-edge count agrees with a host recount of disabled slots.
+    (Final ids can join clusters certified in different rounds: certified
+    clusters get labels smallest - index - 1, which the reference reuses after
+    a round without certificates, and the final partition groups by label as
+    the reference's does: a final id may span instances only through such
+    labels, which is what is checked here.)"""
+    import torch
+
+    off, cols, n, m, starts = B.sbm_batch(count=64, seed=2)
+    off64 = off.to(torch.int64)
+    ids = []
+    for driver, comp in ((P.DRIVER_GRAPH, P.COMPONENTS_AUTO), (P.DRIVER_STREAM, P.COMPONENTS_AUTO),
+                         (P.DRIVER_GRAPH, P.COMPONENTS_PLAIN)):
+        dm = P.CudaDeviceManager(driver=driver, components=comp)
+        dm.initialize_batched_device(n, m, off64.data_ptr(), True, cols.data_ptr(), starts)
+        dm.expanderDecomposition()
+        fp = dm.getFinalPartition()
+        ids.append(fp.clusterIds)
+        if len(ids) == 1:
+            cut_device = dm.getNumCutEdges()
+            final_cols = dm.downloadGraph()[1]
+            labels = dm.downloadLabels()
+        dm.close()
+    np.testing.assert_array_equal(ids[0], ids[1])
+    np.testing.assert_array_equal(ids[0], ids[2])
+    # a final id that spans two instances only ever groups certified labels
+    inst = np.repeat(np.arange(starts.shape[0] - 1), np.diff(starts.astype(np.int64)))
+    lo = np.full(ids[0].max() + 1, np.iinfo(np.int64).max, dtype=np.int64)
+    hi = np.full(ids[0].max() + 1, -1, dtype=np.int64)
+    np.minimum.at(lo, ids[0], inst)
+    np.maximum.at(hi, ids[0], inst)
+    spans = lo[ids[0]] != hi[ids[0]]
+    assert np.all(labels[spans] < 0)
+    valid = int(np.count_nonzero(final_cols != 0xFFFFFFFF))
+    assert cut_device == m - valid // 2
