@@ -84,17 +84,12 @@ def sbm_batch_params(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: f
     return out
 
 
-def sbm_batch(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 1e6, scale: float = 1.0,
-              device: int = 0, segment_len: int = 1 << 24):
-    """Disjoint union of planted-partition instances built on the device:
-    (offsets, cols, n, m, instance_start).  Instance parameters as
-    graphs.sbm_batch; edges drawn on the device (pxr_sbm_edges), so the edge
-    sample differs from the host generator's while following the same
-    distribution (Bernoulli pairs, p_in = d_in / (b - 1), p_out = d_out / (n - b))."""
-    import torch
-    L = _lib.load()
-    dev = torch.device("cuda", device)
-    params = sbm_batch_params(count, seed, n_lo, n_hi, scale)
+def sbm_batch_tasks(params, segment_len: int = 1 << 24):
+    """The work list of the device planted-partition sampler for instances
+    `params` ((n, blocks, d_in, d_out) each, as sbm_batch_params): one task
+    per block pair (SBM_TASK_DTYPE: vertex bases, block sizes, Bernoulli p,
+    intra flag), the first global segment of every task (n_tasks + 1 entries,
+    segments of segment_len candidate pairs), and the instance starts."""
     tasks = []
     starts = [0]
     for n, blocks, d_in, d_out in params:
@@ -119,12 +114,27 @@ def sbm_batch(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 
     nseg = (cand + np.uint64(segment_len - 1)) // np.uint64(segment_len)
     prefix = np.zeros(len(tasks) + 1, dtype=np.uint64)
     np.cumsum(nseg, out=prefix[1:])
+    return T, prefix, starts
+
+
+def sbm_batch(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 1e6, scale: float = 1.0,
+              device: int = 0, segment_len: int = 1 << 24):
+    """Disjoint union of planted-partition instances built on the device:
+    (offsets, cols, n, m, instance_start).  Instance parameters as
+    graphs.sbm_batch; edges drawn on the device (pxr_sbm_edges), so the edge
+    sample differs from the host generator's while following the same
+    distribution (Bernoulli pairs, p_in = d_in / (b - 1), p_out = d_out / (n - b))."""
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda", device)
+    params = sbm_batch_params(count, seed, n_lo, n_hi, scale)
+    T, prefix, starts = sbm_batch_tasks(params, segment_len)
     n_segments = int(prefix[-1])
     d_tasks = torch.from_numpy(T.view(np.uint8).copy()).to(dev)
     d_prefix = torch.from_numpy(prefix.view(np.int64).copy()).to(dev)
     d_count = torch.zeros(max(n_segments, 1), dtype=torch.int32, device=dev)
     stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
-    st = L.pxr_sbm_edges(_p(d_tasks), len(tasks), _p(d_prefix), n_segments, segment_len, seed, _p(d_count), None,
+    st = L.pxr_sbm_edges(_p(d_tasks), len(T), _p(d_prefix), n_segments, segment_len, seed, _p(d_count), None,
                          None, None, stream)
     if st != 0:
         raise _lib.PxrError(st, "pxr_sbm_edges (count)")
@@ -135,7 +145,7 @@ def sbm_batch(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 
     total = int(counts.sum().item()) if n_segments else 0
     u = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
     v = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
-    st = L.pxr_sbm_edges(_p(d_tasks), len(tasks), _p(d_prefix), n_segments, segment_len, seed, None, _p(offs),
+    st = L.pxr_sbm_edges(_p(d_tasks), len(T), _p(d_prefix), n_segments, segment_len, seed, None, _p(offs),
                          _p(u), _p(v), stream)
     if st != 0:
         raise _lib.PxrError(st, "pxr_sbm_edges (write)")

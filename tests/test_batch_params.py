@@ -17,3 +17,23 @@ def test_device_batch_parameters_match_the_host_generator():
     for n, blocks, d_in, d_out in params:
         assert 2 <= blocks <= 64 and blocks <= max(1, n // 2)
         assert 4.0 <= d_in <= 32.0 and 0.1 <= d_out <= 2.0
+
+
+def test_sampler_work_list_covers_every_vertex_pair_once():
+    params = B.sbm_batch_params(count=5, seed=2, n_lo=30, n_hi=300)
+    T, prefix, starts = B.sbm_batch_tasks(params, segment_len=64)
+    su = T["su"].astype(np.int64)
+    sv = T["sv"].astype(np.int64)
+    cand = np.where(T["intra"] == 1, su * (su - 1) // 2, su * sv)
+    # the block pairs of an instance cover its n (n - 1) / 2 vertex pairs exactly
+    inst = np.searchsorted(np.asarray(starts), T["base_u"].astype(np.int64), side="right") - 1
+    for i, (n, blocks, _, _) in enumerate(params):
+        assert int(cand[inst == i].sum()) == n * (n - 1) // 2
+        assert int(np.count_nonzero(inst == i)) == blocks * (blocks + 1) // 2
+    # both blocks of a task lie inside the task's instance
+    end = np.asarray(starts)[inst + 1]
+    assert np.all(T["base_u"].astype(np.int64) + su <= end) and np.all(T["base_v"].astype(np.int64) + sv <= end)
+    # segments: non-decreasing first segments, enough segments for every task's pairs
+    nseg = np.diff(prefix.astype(np.int64))
+    assert np.all(nseg >= 0) and np.all(nseg * 64 >= cand) and np.all((nseg - 1) * 64 < np.maximum(cand, 1))
+    assert np.all(T["p"] > 0) and np.all(T["p"] <= 1)
