@@ -228,6 +228,8 @@ def product_arm(args, rank, world, local_rank):
         off_h = off_d.cpu().pin_memory()
         cols_h = cols_d.cpu().pin_memory()
     off_hn = off_h.numpy().view(np.uint64 if off64 else np.uint32)
+    ids_h = torch.empty(n, dtype=torch.int32).pin_memory()   # the final ids land in page-locked memory
+    ids_hn = ids_h.numpy()
     cols_hn = cols_h.numpy().view(np.uint32)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
@@ -295,7 +297,7 @@ def product_arm(args, rank, world, local_rank):
         # step first: the first transfer from the pinned buffers is slower)
         init_host(dm)
         dm.expanderDecomposition()
-        dm.getFinalPartition()
+        dm.getFinalPartition(out=ids_hn)
         e2e_ms = 0.0
         for _ in range(args.steps):
             flush.zero_()
@@ -306,7 +308,7 @@ def product_arm(args, rank, world, local_rank):
             e0.record(stream)
             init_host(dm)
             dm.expanderDecomposition()
-            fp_e2e = dm.getFinalPartition()
+            fp_e2e = dm.getFinalPartition(out=ids_hn)
             e1.record(stream)
             torch.cuda.synchronize(dev)
             barrier()

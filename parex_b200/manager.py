@@ -172,8 +172,16 @@ class CudaDeviceManager:
         self._call(self._L.pxr_download_partition, _ptr(out), out.shape[0], C.byref(count))
         return out
 
-    def getFinalPartition(self) -> FinalPartition:
-        ids = np.zeros(self.n, dtype=np.int32)
+    def getFinalPartition(self, out: np.ndarray | None = None) -> FinalPartition:
+        """Cluster id of every vertex.  ``out``: an int32 array of n entries
+        to write into (page-locked memory makes the device-to-host copy a
+        direct DMA; a fresh pageable array is allocated otherwise)."""
+        if out is None:
+            ids = np.zeros(self.n, dtype=np.int32)
+        else:
+            if out.dtype != np.int32 or out.shape != (self.n,) or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous int32 array of n entries")
+            ids = out
         k = C.c_int32(0)
         self._call(self._L.pxr_final_partition, _ptr(ids), C.byref(k))
         return FinalPartition(ids, int(k.value))
