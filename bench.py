@@ -208,6 +208,24 @@ def reference_arm(args, rank):
     return 0
 
 
+def max_over_ranks(values, world, device):
+    """Each value's maximum over the ranks (every rank gets it): the job's
+    time is its slowest replica's."""
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_rate(m, world, steps, ms):
+    """Whole-job edges/s: every rank decomposes its own replica of the m-edge
+    graph each step, so the job processes m x world x steps edges in ms."""
+    return m * world * steps / (ms / 1e3)
+
+
 def product_arm(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -325,15 +343,12 @@ def product_arm(args, rank, world, local_rank):
         pst = prof.stats()
         prof_labels_equal = bool(np.array_equal(prof.getFinalPartition().clusterIds, fp.clusterIds))
 
-    times = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms = times.tolist()
+    total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], world, dev)
 
     if rank != 0:
         return 0
-    value = m * world * args.steps / (total_ms / 1e3)
-    e2e_value = m * world * args.steps / (e2e_ms / 1e3)
+    value = job_rate(m, world, args.steps, total_ms)
+    e2e_value = job_rate(m, world, args.steps, e2e_ms)
     h2d = (n + 1) * (8 if off64 else 4) + 2 * m * 4
     d2h = n * 4 + 4
 
