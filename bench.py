@@ -19,8 +19,10 @@ throughput in undirected edges per second (m / step time), summed over ranks.
 * cpu_baseline: the reference's own single-threaded CPU decomposition
   (oracle/_ref/ref_cpu, built from the reference sources) on the same graph.
 
-Multi-GPU: independent replicas, one per rank (the decomposition of one graph
-does not shard); "scaling": "weak".
+Multi-GPU: the decomposition of one graph does not shard, so every rank runs
+its own replica ("scaling": "weak"); the 512-instance batch is split over the
+ranks by expected edges instead (each rank decomposes its shard; the job's
+edges are the shards' sum, "scaling": "strong").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -59,9 +61,10 @@ WORKLOADS = {
 }
 
 
-def load_workload(name, dev=None):
+def load_workload(name, dev=None, rank=0, world=1):
     """(CSRGraph or None, device offsets, device cols, n, m, instance starts or
-    None) for a named workload."""
+    None) for a named workload.  The instance batch is split over the ranks
+    (this rank's shard); the other workloads are replicated."""
     from parex_b200 import graphs as G
     if name.startswith("rmat"):
         from parex_b200 import gpu_build as B
@@ -70,7 +73,8 @@ def load_workload(name, dev=None):
     if name == "batch512":
         import torch
         from parex_b200 import gpu_build as B
-        off_d, cols_d, n, m, starts = B.sbm_batch(512, seed=1, device=dev.index or 0)
+        shard = None if world == 1 else B.shard_instances(B.sbm_batch_params(512, seed=1), world)[rank]
+        off_d, cols_d, n, m, starts = B.sbm_batch(512, seed=1, device=dev.index or 0, instances=shard)
         return None, off_d.to(torch.int64), cols_d, n, m, starts
     g = {"grid128": lambda: G.grid3d(SIDE), "sbm16k": lambda: G.sbm_graph(),
          "regular22": lambda: G.random_regular(1 << 22, 8, seed=1)}[name]()
@@ -220,6 +224,17 @@ def max_over_ranks(values, world, device):
     return t.tolist()
 
 
+def sum_over_ranks(values, world, device):
+    """Each value's sum over the ranks (every rank gets it)."""
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.tolist()
+
+
 def job_rate(m, world, steps, ms):
     """Whole-job edges/s: every rank decomposes its own replica of the m-edge
     graph each step, so the job processes m x world x steps edges in ms."""
@@ -234,7 +249,8 @@ def product_arm(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    g, off_d, cols_d, n, m, starts = load_workload(args.workload, dev)
+    g, off_d, cols_d, n, m, starts = load_workload(args.workload, dev, rank, world)
+    sharded = starts is not None and world > 1   # instances split over the ranks, not replicated
     off64 = off_d is not None and off_d.dtype == torch.int64
     stream = torch.cuda.Stream(device=dev)
     if g is not None:
@@ -344,11 +360,13 @@ def product_arm(args, rank, world, local_rank):
         prof_labels_equal = bool(np.array_equal(prof.getFinalPartition().clusterIds, fp.clusterIds))
 
     total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], world, dev)
+    # edges per step of the whole job: each replica's m, or the shards' sum
+    job_m = int(sum_over_ranks([m], world, dev)[0]) if sharded else m * world
 
     if rank != 0:
         return 0
-    value = job_rate(m, world, args.steps, total_ms)
-    e2e_value = job_rate(m, world, args.steps, e2e_ms)
+    value = job_rate(job_m, 1, args.steps, total_ms)
+    e2e_value = job_rate(job_m, 1, args.steps, e2e_ms)
     h2d = (n + 1) * (8 if off64 else 4) + 2 * m * 4
     d2h = n * 4 + 4
 
@@ -392,11 +410,14 @@ def product_arm(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config((n, m), {"driver": "cuda graph, device-driven round loop", "rounds": rounds,
                                            "clusters": clusters, "cut_edges_device": device_cut,
                                            "sweep_schedule": args.schedule, "row_plan": dm.row_plan(),
-                                           "instances": None if starts is None else int(len(starts) - 1)},
+                                           "instances": None if starts is None else int(len(starts) - 1),
+                                           "parallelism": (f"{world} ranks, instances split by expected edges"
+                                                           if sharded else "replicas"),
+                                           "job_edges_per_step": job_m},
                                   args.workload),
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

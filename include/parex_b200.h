@@ -346,12 +346,14 @@ pxr_status pxr_build_csr(uint32_t n, uint64_t n_edges, const uint32_t* u, const 
                          uint32_t* offsets, uint32_t* cols, uint64_t* m_out, void* stream);
 /* One block pair of a planted-partition instance: candidate pairs
  * (base_u + i, base_v + j), i < su, j < sv (intra: i < j < su, base_u == base_v),
- * each an edge with probability p. */
+ * each an edge with probability p.  key names the task's random stream: a
+ * task's edges depend on (seed, key, su, sv, p) only, not on the task's place
+ * in the list, so a subset of a batch (one shard) draws the same edges. */
 typedef struct {
     uint32_t base_u, base_v, su, sv;
     double p;
     uint32_t intra;
-    uint32_t reserved;
+    uint32_t key;
 } pxr_sbm_task;
 /* Planted-partition edges on the device by geometric skipping: the candidate
  * range of task t is cut into segments of segment_len candidates;

@@ -92,7 +92,7 @@ class ClusterRecord(C.Structure):
 
 
 SBM_TASK_DTYPE = np.dtype([("base_u", "<u4"), ("base_v", "<u4"), ("su", "<u4"), ("sv", "<u4"), ("p", "<f8"),
-                           ("intra", "<u4"), ("reserved", "<u4")])
+                           ("intra", "<u4"), ("key", "<u4")])
 
 
 class MlpLoss(C.Structure):

@@ -139,7 +139,10 @@ __global__ void k_sbm_segments(const pxr_sbm_task* tasks, uint32_t n_tasks, cons
         uint32_t drawn = 0;
         const uint64_t out = seg_offset ? seg_offset[g] : 0;
         if (tk.p > 0.0 && k0 < k1) {
-            uint64_t state = splitmix64(seed ^ splitmix64(g * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull));
+            // the stream of segment (task key, segment within the task)
+            const uint64_t local = g - seg_prefix[lo];
+            const uint64_t sid = ((uint64_t)tk.key << 32) | local;
+            uint64_t state = splitmix64(seed ^ splitmix64(sid * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull));
             const double lq = log1p(-min(tk.p, 1.0 - 1e-16));
             uint64_t k = k0;
             bool first = true;

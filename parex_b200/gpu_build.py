@@ -84,15 +84,21 @@ def sbm_batch_params(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: f
     return out
 
 
-def sbm_batch_tasks(params, segment_len: int = 1 << 24):
+def sbm_batch_tasks(params, segment_len: int = 1 << 24, instances=None):
     """The work list of the device planted-partition sampler for instances
-    `params` ((n, blocks, d_in, d_out) each, as sbm_batch_params): one task
-    per block pair (SBM_TASK_DTYPE: vertex bases, block sizes, Bernoulli p,
-    intra flag), the first global segment of every task (n_tasks + 1 entries,
-    segments of segment_len candidate pairs), and the instance starts."""
+    `params` ((n, blocks, d_in, d_out) each, as sbm_batch_params), or for the
+    subset `instances` of them (a shard): one task per block pair
+    (SBM_TASK_DTYPE: vertex bases, block sizes, Bernoulli p, intra flag, and
+    the key of the task in the whole batch, so a shard draws the same edges),
+    the first global segment of every task (n_tasks + 1 entries, segments of
+    segment_len candidate pairs), and the instance starts."""
+    first_key = np.concatenate([[0], np.cumsum([b * (b + 1) // 2 for _, b, _, _ in params])])
+    chosen = range(len(params)) if instances is None else instances
     tasks = []
     starts = [0]
-    for n, blocks, d_in, d_out in params:
+    for i in chosen:
+        n, blocks, d_in, d_out = params[i]
+        key = int(first_key[i])
         base = starts[-1]
         bsz = n // blocks
         sizes = [bsz] * blocks
@@ -101,14 +107,16 @@ def sbm_batch_tasks(params, segment_len: int = 1 << 24):
         p_in = d_in / max(bsz - 1, 1)
         p_out = d_out / max(n - bsz, 1)
         for a in range(blocks):
-            tasks.append((bstart[a], bstart[a], sizes[a], sizes[a], min(p_in, 1.0), 1))
+            tasks.append((bstart[a], bstart[a], sizes[a], sizes[a], min(p_in, 1.0), 1, key))
+            key += 1
             for b in range(a + 1, blocks):
-                tasks.append((bstart[a], bstart[b], sizes[a], sizes[b], min(p_out, 1.0), 0))
+                tasks.append((bstart[a], bstart[b], sizes[a], sizes[b], min(p_out, 1.0), 0, key))
+                key += 1
         starts.append(base + n)
     T = np.zeros(len(tasks), dtype=_lib.SBM_TASK_DTYPE)
     arr = np.asarray(tasks, dtype=np.float64)
     T["base_u"], T["base_v"] = arr[:, 0], arr[:, 1]
-    T["su"], T["sv"], T["p"], T["intra"] = arr[:, 2], arr[:, 3], arr[:, 4], arr[:, 5]
+    T["su"], T["sv"], T["p"], T["intra"], T["key"] = arr[:, 2], arr[:, 3], arr[:, 4], arr[:, 5], arr[:, 6]
     su, sv = T["su"].astype(np.uint64), T["sv"].astype(np.uint64)
     cand = np.where(T["intra"] == 1, su * (su - np.uint64(1)) // np.uint64(2), su * sv)
     nseg = (cand + np.uint64(segment_len - 1)) // np.uint64(segment_len)
@@ -117,18 +125,34 @@ def sbm_batch_tasks(params, segment_len: int = 1 << 24):
     return T, prefix, starts
 
 
+def shard_instances(params, world: int):
+    """Instances of a batch split over `world` ranks: longest expected edge
+    count first, each to the rank with the fewest expected edges so far
+    (ties to the lower rank); every rank's list in increasing instance order."""
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    weight = [n * (d_in + d_out) / 2.0 for n, _, d_in, d_out in params]
+    for i in sorted(range(len(params)), key=lambda i: (-weight[i], i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        shards[r].append(i)
+        load[r] += weight[i]
+    return [sorted(s) for s in shards]
+
+
 def sbm_batch(count: int = 512, seed: int = 1, n_lo: float = 1e3, n_hi: float = 1e6, scale: float = 1.0,
-              device: int = 0, segment_len: int = 1 << 24):
+              device: int = 0, segment_len: int = 1 << 24, instances=None):
     """Disjoint union of planted-partition instances built on the device:
     (offsets, cols, n, m, instance_start).  Instance parameters as
     graphs.sbm_batch; edges drawn on the device (pxr_sbm_edges), so the edge
     sample differs from the host generator's while following the same
-    distribution (Bernoulli pairs, p_in = d_in / (b - 1), p_out = d_out / (n - b))."""
+    distribution (Bernoulli pairs, p_in = d_in / (b - 1), p_out = d_out / (n - b)).
+    `instances`: build only these instances of the batch (a shard; each draws
+    the same edges as in the whole batch)."""
     import torch
     L = _lib.load()
     dev = torch.device("cuda", device)
     params = sbm_batch_params(count, seed, n_lo, n_hi, scale)
-    T, prefix, starts = sbm_batch_tasks(params, segment_len)
+    T, prefix, starts = sbm_batch_tasks(params, segment_len, instances)
     n_segments = int(prefix[-1])
     d_tasks = torch.from_numpy(T.view(np.uint8).copy()).to(dev)
     d_prefix = torch.from_numpy(prefix.view(np.int64).copy()).to(dev)

@@ -37,3 +37,31 @@ def test_sampler_work_list_covers_every_vertex_pair_once():
     nseg = np.diff(prefix.astype(np.int64))
     assert np.all(nseg >= 0) and np.all(nseg * 64 >= cand) and np.all((nseg - 1) * 64 < np.maximum(cand, 1))
     assert np.all(T["p"] > 0) and np.all(T["p"] <= 1)
+
+
+def test_shards_partition_the_batch_and_balance_expected_edges():
+    params = B.sbm_batch_params(count=512, seed=1)
+    weight = np.array([n * (a + b) / 2 for n, _, a, b in params])
+    for world in (1, 2, 4, 8):
+        shards = B.shard_instances(params, world)
+        assert len(shards) == world
+        allidx = np.sort(np.concatenate([np.asarray(s, dtype=np.int64) for s in shards]))
+        np.testing.assert_array_equal(allidx, np.arange(512))
+        loads = np.array([weight[s].sum() for s in shards])
+        assert loads.max() - loads.min() <= weight.max() + 1e-6   # greedy bound
+        assert shards == B.shard_instances(params, world)          # deterministic
+
+
+def test_a_shard_holds_the_same_tasks_as_the_whole_batch():
+    params = B.sbm_batch_params(count=6, seed=4, n_lo=40, n_hi=400)
+    T, _, starts = B.sbm_batch_tasks(params, 64)
+    Ts, _, starts_s = B.sbm_batch_tasks(params, 64, instances=[1, 4])
+    full_inst = np.searchsorted(np.asarray(starts), T["base_u"].astype(np.int64), side="right") - 1
+    sub = T[np.isin(full_inst, [1, 4])]
+    for f in ("su", "sv", "p", "intra", "key"):
+        np.testing.assert_array_equal(Ts[f], sub[f])
+    # vertex bases move with the instance's place in the shard
+    n1 = params[1][0]
+    off = np.where(np.arange(len(sub)) < np.count_nonzero(full_inst == 1), starts[1], starts[4] - n1)
+    np.testing.assert_array_equal(Ts["base_u"].astype(np.int64), sub["base_u"].astype(np.int64) - off)
+    assert starts_s == [0, n1, n1 + params[4][0]]

@@ -1,8 +1,9 @@
-"""bench.py on N ranks (replicas): every rank times its own decomposition,
-the job's time is the maximum over the ranks, and the whole-job rate counts
-every rank's edges.  Checked here with two gloo ranks on the CPU (the same
-collective calls bench.py makes over NCCL on GPUs); the reference arm runs
-on rank 0 only.
+"""bench.py on N ranks: every rank times its own decomposition (a replica,
+or its shard of the instance batch), the job's time is the maximum over the
+ranks, and the whole-job rate counts every rank's edges (replicas: m per
+rank; shards: the sum of the shards' edges).  Checked here with two gloo
+ranks on the CPU (the same collective calls bench.py makes over NCCL on
+GPUs); the reference arm runs on rank 0 only.
 """
 import argparse
 import os
@@ -35,6 +36,8 @@ def _rank_main(rank, world, port, out):
     try:
         # rank r timed 100 + 10 r ms for the device steps and 200 - 10 r ms end to end
         got = bench.max_over_ranks([100.0 + 10 * rank, 200.0 - 10 * rank], world, "cpu")
+        # and rank r holds a shard of 1000 + r edges: the job's edges are their sum
+        got += bench.sum_over_ranks([1000.0 + rank], world, "cpu")
         out.put((rank, got))
         dist.barrier()
     finally:
@@ -52,7 +55,7 @@ def test_two_ranks_agree_on_the_slowest_replica():
         p.join(timeout=120)
         assert p.exitcode == 0
     res = dict(out.get(timeout=10) for _ in range(world))
-    assert res[0] == res[1] == [110.0, 200.0]
+    assert res[0] == res[1] == [110.0, 200.0, 2001.0]
 
 
 def test_job_rate_counts_every_replica():

@@ -135,3 +135,19 @@ def test_device_batch_at_scale_size_independent_properties():
     assert np.all(labels[spans] < 0)
     valid = int(np.count_nonzero(final_cols != 0xFFFFFFFF))
     assert cut_device == m - valid // 2
+
+
+def test_a_shard_draws_the_same_edges_as_the_whole_batch():
+    off, cols, n, m, starts = B.sbm_batch(count=8, seed=5, n_lo=200, n_hi=3000)
+    offs, colss, ns, ms, starts_s = B.sbm_batch(count=8, seed=5, n_lo=200, n_hi=3000, instances=[2, 6])
+    g, gs = B.to_host(off, cols), B.to_host(offs, colss)
+
+    def rows(graph, lo, hi):
+        o = graph.offsets.astype(np.int64)
+        return o[lo:hi + 1] - o[lo], graph.cols[o[lo]:o[hi]].astype(np.int64) - lo
+
+    for k, i in enumerate((2, 6)):
+        a_off, a_cols = rows(g, int(starts[i]), int(starts[i + 1]))
+        b_off, b_cols = rows(gs, int(starts_s[k]), int(starts_s[k + 1]))
+        np.testing.assert_array_equal(a_off, b_off)
+        np.testing.assert_array_equal(a_cols, b_cols)
