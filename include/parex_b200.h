@@ -284,6 +284,27 @@ pxr_status pxr_download_degrees(pxr_handle* h, uint32_t* out);
 pxr_status pxr_download_labels(pxr_handle* h, int32_t* out);
 /* CudaDeviceManager::downloadActiveEdgeMap() (cuda/interface.h:44): 2m ints. */
 pxr_status pxr_active_edge_map(pxr_handle* h, int32_t* out);
+/* Cut edges of the current partition, recounted on the device: undirected
+ * edges of the graph as uploaded whose ends carry different labels, i.e.
+ * different getFinalPartition ids.  This is the count the reference's
+ * application makes on the host after getFinalPartition
+ * (Partition::splitByIndices and getNumCutEdges, main.cpp:54-60), which the
+ * library's getNumCutEdges (m - valid/2, cuda/devPartition.h:741-759) does
+ * not give once clusters are certified (their rows are no longer updated).
+ * PXR_INVALID_ARG after pxr_set_state loaded disabled slots, whose
+ * neighbours are unknown. */
+pxr_status pxr_count_cut_edges(pxr_handle* h, uint64_t* out);
+/* Certificate record, n uint32 (no counterpart in the reference, which
+ * keeps none).  0 while the vertex is active.  When its cluster is certified
+ * - deactivated by the keep test (potential spread below rw_threshold or
+ * fewer than 2 vertices, cuda/devPartition.h:173-184) - the round in which
+ * that happened, plus 1, with bit 31 set when the certified set is not the
+ * whole set swept in that round (the swept cluster was cut, or fell apart
+ * into components).  A certified vertex neither walks nor recentres again,
+ * so pxr_read_potentials returns the potentials the keep test saw; with the
+ * final partition this lets a caller re-check every certificate
+ * (parex_b200/certificate.py). */
+pxr_status pxr_download_certificates(pxr_handle* h, uint32_t* out);
 /* CudaDeviceManager::getNumClusters() (cuda/interface.h:46; the reference
  * returns 0 unconditionally, cuda/device.h:120-123): here the number of
  * active clusters. */

@@ -60,11 +60,15 @@ def lib():
                      "orc_n_data_clusters"]:
             getattr(L, name).argtypes = [p]
             getattr(L, name).restype = C.c_uint32
+        L.orc_rmat_csr.argtypes = [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, p,
+                                   C.POINTER(p), C.POINTER(C.c_uint64)]
+        L.orc_rmat_csr.restype = C.c_int
+        L.orc_free.argtypes = [p]
         L.orc_smallest_label.argtypes = [p]
         L.orc_smallest_label.restype = C.c_int32
         for name in ["orc_labels", "orc_active", "orc_internal_degrees", "orc_cols", "orc_keys",
                      "orc_sorted", "orc_sweep_labels", "orc_sweep_volumes", "orc_all_cuts",
-                     "orc_cuts", "orc_data_labels", "orc_cluster_values"]:
+                     "orc_cuts", "orc_data_labels", "orc_cluster_values", "orc_certificates"]:
             getattr(L, name).argtypes = [p]
             getattr(L, name).restype = p
         _lib = L
@@ -89,6 +93,27 @@ def initial_potentials(offsets: np.ndarray, seed: int) -> np.ndarray:
     out = np.zeros(n, dtype=np.float32)
     lib().orc_initial_potentials(n, _ptr(off), seed, _ptr(out))
     return out
+
+
+def rmat_csr(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 1):
+    """R-MAT CSR (offsets uint64[n+1], cols uint32[2m]) built on the host in C
+    (oracle/graph_gen.c): the graph of parex_b200.graphs.rmat and of the
+    library's device generator, without loading the library."""
+    n = 1 << scale
+    ta, tab, tabc = (int(round(t * 65536)) for t in (a, a + b, a + b + c))
+    off = np.zeros(n + 1, dtype=np.uint64)
+    cols_p = C.c_void_p()
+    m = C.c_uint64(0)
+    if lib().orc_rmat_csr(scale, edge_factor << scale, ta, tab, tabc, seed, _ptr(off), C.byref(cols_p),
+                          C.byref(m)) != 0:
+        raise MemoryError("orc_rmat_csr: out of host memory")
+    try:
+        cols = np.ctypeslib.as_array((C.c_uint32 * (2 * m.value)).from_address(cols_p.value)).copy() \
+            if m.value else np.zeros(0, dtype=np.uint32)
+    finally:
+        lib().orc_free(cols_p)
+    return off, cols
 
 
 class Oracle:
@@ -181,3 +206,4 @@ class Oracle:
     def cuts(self): return _view(lib().orc_cuts(self._s), SWEEP_CUT, self.n_cuts)
     def data_labels(self): return _view(lib().orc_data_labels(self._s), np.int32, self.n_data_clusters)
     def cluster_values(self): return _view(lib().orc_cluster_values(self._s), CLUSTER_DATA, self.n_data_clusters)
+    def certificates(self): return _view(lib().orc_certificates(self._s), np.uint32, self.n).copy()

@@ -48,6 +48,16 @@ struct orc_state {
     uint32_t k_data;
     uint32_t* parent;
     uint32_t* tmp_u32;
+    /* certificate record (no reference counterpart): per vertex, the round in
+     * which its cluster was certified (+1) with bit 31 set when the certified
+     * set is not the whole set swept that round (cut, or split into
+     * components); 0 while active.  sweep_of / sweep_cnt / sweep_cut hold the
+     * last sweep's cluster of each vertex, its size and its cut decision. */
+    uint32_t* cert;
+    int32_t* sweep_of;
+    uint32_t* sweep_cnt;
+    uint8_t* sweep_cut;
+    uint32_t round;
 };
 
 static void* xcalloc(size_t count, size_t size) {
@@ -181,6 +191,10 @@ orc_state* orc_create(uint32_t n, uint64_t m, const uint64_t* offsets, const uin
     s->csum_fixed_avg = (double*)xcalloc(n, 8);
     s->parent = (uint32_t*)xcalloc(n, 4);
     s->tmp_u32 = (uint32_t*)xcalloc(n, 4);
+    s->cert = (uint32_t*)xcalloc(n, 4);
+    s->sweep_of = (int32_t*)xcalloc(n, 4);
+    s->sweep_cnt = (uint32_t*)xcalloc(n, 4);
+    s->sweep_cut = (uint8_t*)xcalloc(n, 1);
     uint64_t maxdeg = 0;
     for (uint32_t v = 0; v < n; ++v) {
         const uint64_t d = offsets[v + 1] - offsets[v];
@@ -189,6 +203,7 @@ orc_state* orc_create(uint32_t n, uint64_t m, const uint64_t* offsets, const uin
         s->act[v].nix = v;                           /* MakeLabeledNodeOp */
         s->act[v].label = 0;
         s->lookup[v] = -1;
+        s->sweep_of[v] = -1;
     }
     uint64_t big = maxdeg > n ? maxdeg : n;
     uint32_t bits = 0;
@@ -206,7 +221,7 @@ void orc_destroy(orc_state* s) {
     void* ptrs[] = {s->off, s->cols, s->labels, s->ideg, s->xd[0], s->xd[1], s->xf, s->xt,
                     s->act, s->keys, s->nd, s->sorted, s->ulabels, s->vols, s->lookup,
                     s->allcuts, s->cuts, s->clabels, s->cdata, s->csum_fixed_avg, s->parent,
-                    s->tmp_u32};
+                    s->tmp_u32, s->cert, s->sweep_of, s->sweep_cnt, s->sweep_cut};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
     free(s);
 }
@@ -328,12 +343,32 @@ void orc_walk(orc_state* s) {
 /* sweep: SweepCutManager::prepare_nodes + compute_sweep_cuts,
  * cuda/devSweepCut.h:20-112, 469-730                                        */
 
-static const uint64_t* g_sort_keys;
-static int cmp_key_index(const void* a, const void* b) {
-    const uint32_t ia = *(const uint32_t*)a, ib = *(const uint32_t*)b;
-    const uint64_t ka = g_sort_keys[ia], kb = g_sort_keys[ib];
-    if (ka != kb) return ka < kb ? -1 : 1;
-    return ia < ib ? -1 : (ia > ib);             /* stable */
+/* perm = the stable ascending order of keys[0..n): an LSD radix sort of
+ * (key, index) on 16-bit digits, skipping digits that are equal in every key
+ * (the result is that of a stable comparison sort, as CUB's radix sort and
+ * thrust::stable_sort give). */
+static void stable_order_u64(const uint64_t* keys, uint32_t n, uint32_t* perm) {
+    for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+    if (n < 2) return;
+    uint64_t all_or = 0, all_and = ~0ull;
+    for (uint32_t i = 0; i < n; ++i) { all_or |= keys[i]; all_and &= keys[i]; }
+    const uint64_t varying = all_or ^ all_and;
+    uint32_t* tmp = (uint32_t*)xcalloc(n, 4);
+    uint32_t* cnt = (uint32_t*)xcalloc(65536, 4);
+    uint32_t* src = perm;
+    uint32_t* dst = tmp;
+    for (unsigned shift = 0; shift < 64; shift += 16) {
+        if (((varying >> shift) & 0xFFFFull) == 0) continue;
+        memset(cnt, 0, 65536 * 4);
+        for (uint32_t i = 0; i < n; ++i) cnt[(keys[src[i]] >> shift) & 0xFFFF]++;
+        uint32_t sum = 0;
+        for (uint32_t d = 0; d < 65536; ++d) { const uint32_t c = cnt[d]; cnt[d] = sum; sum += c; }
+        for (uint32_t i = 0; i < n; ++i) dst[cnt[(keys[src[i]] >> shift) & 0xFFFF]++] = src[i];
+        uint32_t* t = src; src = dst; dst = t;
+    }
+    if (src != perm) memcpy(perm, src, (size_t)n * 4);
+    free(tmp);
+    free(cnt);
 }
 
 void orc_sweep(orc_state* s) {
@@ -359,9 +394,7 @@ void orc_sweep(orc_state* s) {
     }
     /* cub::DeviceRadixSort::SortPairs: stable by the 64-bit key */
     uint32_t* perm = (uint32_t*)xcalloc(nA, 4);
-    for (uint32_t i = 0; i < nA; ++i) perm[i] = i;
-    g_sort_keys = s->keys;
-    qsort(perm, nA, 4, cmp_key_index);
+    stable_order_u64(s->keys, nA, perm);
     uint64_t* skeys = (uint64_t*)xcalloc(nA, 8);
     orc_node_data* snd = (orc_node_data*)xcalloc(nA, sizeof(orc_node_data));
     for (uint32_t i = 0; i < nA; ++i) { skeys[i] = s->keys[perm[i]]; snd[i] = s->nd[perm[i]]; }
@@ -415,9 +448,20 @@ void orc_sweep(orc_state* s) {
     }
     /* copy_if(CheckThreshold) */
     uint32_t nc = 0;
-    for (uint32_t j = 0; j < k; ++j)
-        if ((double)s->allcuts[j].sparsity < (double)s->sc_threshold) s->cuts[nc++] = s->allcuts[j];
+    for (uint32_t j = 0; j < k; ++j) {
+        const int cut = (double)s->allcuts[j].sparsity < (double)s->sc_threshold;
+        if (cut) s->cuts[nc++] = s->allcuts[j];
+        s->sweep_cut[j] = (uint8_t)cut;
+        s->sweep_cnt[j] = 0;
+    }
     s->n_cut = nc;
+    /* certificate record: the swept cluster of every vertex and its size */
+    c = 0;
+    for (uint32_t i = 0; i < na; ++i) {
+        if (i > 0 && s->act[i - 1].label != s->act[i].label) ++c;
+        s->sweep_of[s->act[i].nix] = (int32_t)c;
+        s->sweep_cnt[c] += 1;
+    }
     free(skeys);
     free(snd);
 }
@@ -481,21 +525,14 @@ void orc_components_stage(orc_state* s) {
 /* ------------------------------------------------------------------------ */
 /* PartitionManager::computeClusterData, cuda/devPartition.h:380-411          */
 
-static const orc_lnode* g_sort_act;
-static int cmp_label_index(const void* a, const void* b) {
-    const uint32_t ia = *(const uint32_t*)a, ib = *(const uint32_t*)b;
-    const int32_t la = g_sort_act[ia].label, lb = g_sort_act[ib].label;
-    if (la != lb) return la < lb ? -1 : 1;
-    return ia < ib ? -1 : (ia > ib);
-}
-
 void orc_cluster_data_stage(orc_state* s) {
     const uint32_t nA = s->n_act;
     /* stable_sort(LabeledNodeLabelLess) */
     uint32_t* perm = (uint32_t*)xcalloc(nA, 4);
-    for (uint32_t i = 0; i < nA; ++i) perm[i] = i;
-    g_sort_act = s->act;
-    qsort(perm, nA, 4, cmp_label_index);
+    uint64_t* lkey = (uint64_t*)xcalloc(nA, 8);
+    for (uint32_t i = 0; i < nA; ++i) lkey[i] = (uint64_t)((uint32_t)s->act[i].label ^ 0x80000000u);
+    stable_order_u64(lkey, nA, perm);
+    free(lkey);
     orc_lnode* sorted = (orc_lnode*)xcalloc(nA, sizeof(orc_lnode));
     for (uint32_t i = 0; i < nA; ++i) sorted[i] = s->act[perm[i]];
     memcpy(s->act, sorted, (size_t)nA * sizeof(orc_lnode));
@@ -537,6 +574,18 @@ void orc_cluster_data_stage(orc_state* s) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* Certificate record of a vertex whose cluster is certified (deactivated) now:
+ * the round, and whether the certified set (count vertices) is exactly the
+ * set swept this round - only then does that sweep's "no cut below sc" speak
+ * for it.  No reference counterpart: the reference keeps no such record.    */
+
+static void certify_vertex(orc_state* s, uint32_t v, uint32_t count) {
+    const int32_t c = s->sweep_of[v];
+    const int whole = c >= 0 && !s->sweep_cut[c] && s->sweep_cnt[c] == count;
+    s->cert[v] = (s->round + 1u) | (whole ? 0u : 0x80000000u);
+}
+
+/* ------------------------------------------------------------------------ */
 /* PartitionManager::recenterAndDeactivateClusters, cuda/devPartition.h:624-711 */
 
 void orc_recenter_stage(orc_state* s) {
@@ -561,6 +610,7 @@ void orc_recenter_stage(orc_state* s) {
             const int32_t nl = s->smallest - c - 1;
             s->act[i].label = nl;
             s->labels[v] = nl;
+            certify_vertex(s, v, cd.count);
         } else {
             s->act[i].label = newlab[c];
             s->labels[v] = newlab[c];
@@ -613,6 +663,7 @@ void orc_cut_clusters(orc_state* s) {
     orc_cluster_data_stage(s);
     orc_recenter_stage(s);
     orc_disable_stage(s);
+    s->round += 1;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -707,7 +758,10 @@ void orc_scheduled_round(orc_state* s, const uint8_t* due) {
         const int32_t nl = data_nl[c];
         s->act[i].label = nl;
         s->labels[v] = nl;
-        if (nl < 0) continue;
+        if (nl < 0) {
+            certify_vertex(s, v, s->cdata[c].count);
+            continue;
+        }
         if (s->mode == ORC_MODE_REF) {
             const double avg = (double)s->cdata[c].sum / (double)s->cdata[c].count;
             s->xd[s->cur][v] -= avg;
@@ -733,6 +787,7 @@ void orc_scheduled_round(orc_state* s, const uint8_t* due) {
     memcpy(s->act + s->n_act, carried, (size_t)nc * sizeof(orc_lnode));
     s->n_act += nc;
     s->n_clusters = (uint32_t)survivors;
+    s->round += 1;
     free(carried); free(croot); free(root_of); free(order); free(data_nl); free(carried_nl); free(carried_label);
 }
 
@@ -798,3 +853,4 @@ const orc_sweep_cut* orc_all_cuts(const orc_state* s) { return s->allcuts; }
 const orc_sweep_cut* orc_cuts(const orc_state* s) { return s->cuts; }
 const int32_t* orc_data_labels(const orc_state* s) { return s->clabels; }
 const orc_cluster_data* orc_cluster_values(const orc_state* s) { return s->cdata; }
+const uint32_t* orc_certificates(const orc_state* s) { return s->cert; }

@@ -104,6 +104,10 @@ const orc_sweep_cut* orc_all_cuts(const orc_state* s);
 const orc_sweep_cut* orc_cuts(const orc_state* s);
 const int32_t* orc_data_labels(const orc_state* s);
 const orc_cluster_data* orc_cluster_values(const orc_state* s);
+/* Certificate record per vertex (no reference counterpart): 0 while the
+ * vertex is active; once its cluster is certified, (round + 1) with bit 31
+ * set when the certified set differs from the set swept in that round. */
+const uint32_t* orc_certificates(const orc_state* s);
 /* current potentials widened to double */
 void orc_get_potentials(const orc_state* s, double* out);
 

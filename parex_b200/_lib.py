@@ -28,7 +28,7 @@ SYMBOLS = [
     "pxr_cut_clusters", "pxr_decompose", "pxr_read_potentials", "pxr_read_sweep_cuts",
     "pxr_download_partition", "pxr_final_partition", "pxr_num_cut_edges", "pxr_download_graph",
     "pxr_download_graph64", "pxr_download_degrees", "pxr_download_labels", "pxr_active_edge_map",
-    "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
+    "pxr_count_cut_edges", "pxr_download_certificates", "pxr_num_active_clusters", "pxr_get_stats", "pxr_set_profiling", "pxr_phase_stats",
     "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
     "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
@@ -161,6 +161,8 @@ def load() -> C.CDLL:
     L.pxr_download_degrees.argtypes = [p, p]
     L.pxr_download_labels.argtypes = [p, p]
     L.pxr_active_edge_map.argtypes = [p, p]
+    L.pxr_count_cut_edges.argtypes = [p, C.POINTER(u64)]
+    L.pxr_download_certificates.argtypes = [p, p]
     L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]
     L.pxr_get_stats.argtypes = [p, C.POINTER(Stats)]
     L.pxr_final_partition_static.argtypes = [p, u32, p, p, p]

@@ -8,6 +8,11 @@
 namespace pxr {
 
 constexpr uint32_t kInvalidEdge = 0xFFFFFFFFu;
+// A disabled CSR slot keeps its neighbour with the top bit set (vertex ids
+// are below 2^31 - 1), so the graph as uploaded stays recoverable on the
+// device; downloads show the reference's INVALID_EDGE there.
+constexpr uint32_t kDisabledBit = 0x80000000u;
+__host__ __device__ __forceinline__ bool slot_valid(uint32_t c) { return c < kDisabledBit; }
 constexpr uint32_t kNoCut = 0xFFFFFFFFu;
 
 // Device-side error bits, OR-ed into RoundCtr::err.

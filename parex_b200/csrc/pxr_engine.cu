@@ -79,10 +79,69 @@ __global__ void __launch_bounds__(kBlock) k_fp_rank(const uint32_t* keys0, const
 __global__ void k_count_valid(const uint32_t* cols, uint64_t slots, unsigned long long* out) {
     uint32_t c = 0;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < slots; j += (uint64_t)gridDim.x * blockDim.x)
-        c += cols[j] != kInvalidEdge;
+        c += slot_valid(cols[j]);
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
     if ((threadIdx.x & 31u) == 0 && c) atomicAdd(out, (unsigned long long)c);
 }
+
+// Cut edges of the partition given by the labels: CSR slots (both directions
+// of every edge) whose ends carry different labels, over the graph as
+// uploaded (a disabled slot still holds its neighbour under kDisabledBit).
+// Final ids are a bijection of label values, so these are the edges whose
+// ends carry different final ids.  A tile of kCountTile slots finds its
+// first and last rows once; each slot's row is then a binary search between
+// them.  bad is set when a slot's neighbour is unknown (pxr_set_state may
+// load disabled slots without one).
+constexpr uint32_t kCountTile = 4096;
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_count_cut(const OffT* off, const uint32_t* cols, const int32_t* lab,
+                                                      uint32_t n, uint64_t slots, unsigned long long* out,
+                                                      uint32_t* bad) {
+    __shared__ uint32_t s_rows[2];
+    __shared__ unsigned long long s_sum[kBlock / 32];
+    const uint64_t ntiles = (slots + kCountTile - 1) / kCountTile;
+    unsigned long long cnt = 0;
+    uint32_t unknown = 0;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t s0 = tile * kCountTile;
+        const uint64_t s1 = s0 + kCountTile < slots ? s0 + kCountTile : slots;
+        if (threadIdx.x < 2) {
+            // last row r with off[r] <= target (rows are non-decreasing, off[n] = slots > target)
+            const uint64_t target = threadIdx.x == 0 ? s0 : s1 - 1;
+            uint32_t lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo + 1) / 2;
+                if ((uint64_t)off[mid] <= target) lo = mid; else hi = mid - 1;
+            }
+            s_rows[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        const uint32_t r0 = s_rows[0], r1 = s_rows[1];
+        __syncthreads();
+        for (uint64_t sl = s0 + threadIdx.x; sl < s1; sl += blockDim.x) {
+            uint32_t lo = r0, hi = r1;
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo + 1) / 2;
+                if ((uint64_t)off[mid] <= sl) lo = mid; else hi = mid - 1;
+            }
+            const uint32_t u = cols[sl] & ~kDisabledBit;
+            if (u >= n) { unknown = 1; continue; }
+            cnt += lab[lo] != lab[u] ? 1ull : 0ull;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+    if ((threadIdx.x & 31u) == 0) s_sum[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kBlock / 32; ++w) t += s_sum[w];
+        if (t) atomicAdd(out, t);
+    }
+    if (unknown) atomicOr(bad, 1u);
+}
+
 
 template <typename OffT>
 __global__ void k_degrees(const OffT* off, uint32_t n, uint32_t* ideg, int32_t* lab, uint32_t* act, uint32_t* ids) {
@@ -116,7 +175,7 @@ __global__ void k_batch_setup(const OffT* off, const uint32_t* cols, const uint3
             bool out = false;
             for (OffT e = off[v]; e < off[v + 1]; ++e) {
                 const uint32_t u = cols[e];
-                out |= u != kInvalidEdge && (u < a || u >= b);
+                out |= slot_valid(u) && (u < a || u >= b);
             }
             if (out) atomicOr(bad, 1u);
         }
@@ -262,6 +321,7 @@ struct pxr_handle {
     int64_t* acc_sum = nullptr;
     int32_t* newlab = nullptr;
     double* avg = nullptr;
+    uint32_t* cert = nullptr;
     int32_t* pdif = nullptr;
     uint32_t* pvol = nullptr;
     uint32_t* act[2] = {nullptr, nullptr};
@@ -392,6 +452,7 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.acc_cnt = h->acc_cnt;
     d.newlab = h->newlab;
     d.avg = h->avg;
+    d.cert = h->cert;
     d.pdif = h->pdif;
     d.pvol = h->pvol;
     d.cut_off = h->cut_off;
@@ -915,7 +976,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->cols, std::max<uint64_t>(h->slots, 1));
     A(&h->lab, N); A(&h->ideg, N); A(&h->x, N); A(&h->xt[0], N); A(&h->xt[1], N);
     A(&h->dv, N); A(&h->parent, N); A(&h->acc_max, N); A(&h->acc_min, N); A(&h->acc_cnt, N);
-    A(&h->acc_sum, N); A(&h->newlab, N); A(&h->avg, N); A(&h->pdif, N); A(&h->pvol, N);
+    A(&h->acc_sum, N); A(&h->newlab, N); A(&h->avg, N); A(&h->pdif, N); A(&h->pvol, N); A(&h->cert, N);
     for (int i = 0; i < 2; ++i) {
         A(&h->act[i], N); A(&h->ids[i], N); A(&h->par[i], N); A(&h->keys[i], N); A(&h->vals[i], N); A(&h->roots[i], N);
         A(&h->tab[i].start, N); A(&h->tab[i].size, N); A(&h->tab[i].vol, N); A(&h->tab[i].vol_start, N);
@@ -1191,6 +1252,7 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     c.max_parent = 0xFFFFFFFFu;   // the first round sorts globally (the list is in vertex order)
     c.max_csize = n;
     PXR_CUDA(h, cudaMemcpyAsync(h->ctr, &c, sizeof(RoundCtr), cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->cert, 0, (size_t)std::max<uint32_t>(n, 1) * 4, s));
     if (n) {
         k_degrees<OffT><<<grid_for(n), kBlock, 0, s>>>(static_cast<const OffT*>(h->off), n, h->ideg, h->lab,
                                                       h->act[0], h->ids[0]);
@@ -1544,6 +1606,23 @@ pxr_status pxr_num_cut_edges(pxr_handle* h, uint64_t* out) {
     return PXR_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// The CSR columns into host memory with disabled slots as INVALID_EDGE (the
+// reference's mutated graph).
+pxr_status download_cols(pxr_handle* h, uint32_t* cols) {
+    if (!h->slots) return PXR_OK;
+    PXR_CUDA(h, cudaMemcpyAsync(cols, h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (uint64_t j = 0; j < h->slots; ++j)
+        if (!slot_valid(cols[j])) cols[j] = PXR_INVALID_EDGE;
+    return PXR_OK;
+}
+}  // namespace
+
+extern "C" {
+
 pxr_status pxr_download_graph64(pxr_handle* h, uint64_t* offsets, uint32_t* cols) {
     if (!h || !offsets || (h->slots && !cols)) return PXR_INVALID_ARG;
     if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
@@ -1555,9 +1634,8 @@ pxr_status pxr_download_graph64(pxr_handle* h, uint64_t* offsets, uint32_t* cols
         PXR_CUDA(h, cudaStreamSynchronize(h->stream));
         for (size_t i = 0; i < o.size(); ++i) offsets[i] = o[i];
     }
-    if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(cols, h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
     PXR_CUDA(h, cudaStreamSynchronize(h->stream));
-    return PXR_OK;
+    return download_cols(h, cols);
 }
 
 pxr_status pxr_download_graph(pxr_handle* h, uint32_t* offsets, uint32_t* cols) {
@@ -1565,9 +1643,8 @@ pxr_status pxr_download_graph(pxr_handle* h, uint32_t* offsets, uint32_t* cols) 
     if (h->off64) return fail(h, PXR_INVALID_ARG, "graph has 64-bit offsets");
     if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
     PXR_CUDA(h, cudaMemcpyAsync(offsets, h->off, ((size_t)h->n + 1) * 4, cudaMemcpyDeviceToHost, h->stream));
-    if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(cols, h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
     PXR_CUDA(h, cudaStreamSynchronize(h->stream));
-    return PXR_OK;
+    return download_cols(h, cols);
 }
 
 pxr_status pxr_download_degrees(pxr_handle* h, uint32_t* out) {
@@ -1592,7 +1669,41 @@ pxr_status pxr_active_edge_map(pxr_handle* h, int32_t* out) {
     std::vector<uint32_t> c(h->slots);
     if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(c.data(), h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
     PXR_CUDA(h, cudaStreamSynchronize(h->stream));
-    for (uint64_t j = 0; j < h->slots; ++j) out[j] = c[j] != PXR_INVALID_EDGE ? 1 : 0;
+    for (uint64_t j = 0; j < h->slots; ++j) out[j] = slot_valid(c[j]) ? 1 : 0;
+    return PXR_OK;
+}
+
+pxr_status pxr_download_certificates(pxr_handle* h, uint32_t* out) {
+    if (!h || (h->n && !out)) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    if (h->n) PXR_CUDA(h, cudaMemcpyAsync(out, h->cert, (size_t)h->n * 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    return PXR_OK;
+}
+
+pxr_status pxr_count_cut_edges(pxr_handle* h, uint64_t* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    if (!h->initialized) return fail(h, PXR_NOT_INITIALIZED, "no graph uploaded");
+    unsigned long long both = 0;
+    uint32_t bad = 0;
+    PXR_CUDA(h, cudaMemsetAsync(h->d_valid, 0, 8, h->stream));
+    PXR_CUDA(h, cudaMemsetAsync(h->d_check, 0, 4, h->stream));
+    if (h->slots) {
+        const uint32_t grid = (uint32_t)std::min<uint64_t>((h->slots + kCountTile - 1) / kCountTile, 148u * 16u);
+        if (h->off64)
+            k_count_cut<uint64_t><<<grid, kBlock, 0, h->stream>>>(static_cast<const uint64_t*>(h->off), h->cols,
+                                                                  h->lab, h->n, h->slots, h->d_valid, h->d_check);
+        else
+            k_count_cut<uint32_t><<<grid, kBlock, 0, h->stream>>>(static_cast<const uint32_t*>(h->off), h->cols,
+                                                                  h->lab, h->n, h->slots, h->d_valid, h->d_check);
+        ++h->launches;
+    }
+    PXR_CUDA(h, cudaGetLastError());
+    PXR_CUDA(h, cudaMemcpyAsync(&both, h->d_valid, 8, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaMemcpyAsync(&bad, h->d_check, 4, cudaMemcpyDeviceToHost, h->stream));
+    PXR_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (bad) return fail(h, PXR_INVALID_ARG, "a disabled slot's neighbour is unknown (slots loaded by pxr_set_state)");
+    *out = both / 2;
     return PXR_OK;
 }
 
@@ -1708,6 +1819,7 @@ pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* a
     }
     PXR_CUDA(h, cudaMemcpyAsync(h->ideg, ideg, (size_t)n * 4, cudaMemcpyHostToDevice, s));
     if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(h->cols, cols, h->slots * 4, cudaMemcpyHostToDevice, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->cert, 0, (size_t)std::max<uint32_t>(n, 1) * 4, s));
     if (n_clusters) {
         PXR_CUDA(h, cudaMemcpyAsync(t.start, start.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));
         PXR_CUDA(h, cudaMemcpyAsync(t.size, size.data(), n_clusters * 4ull, cudaMemcpyHostToDevice, s));

@@ -317,11 +317,11 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
             for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? stream_col(d.cols + s + u * W) : kInvalidEdge;
             float xv[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) xv[u] = nb[u] != kInvalidEdge ? xt_in[nb[u]] : 0.0f;
+            for (int u = 0; u < kSlotUnroll; ++u) xv[u] = slot_valid(nb[u]) ? xt_in[nb[u]] : 0.0f;
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) {
                 st_s += s + u * W < end ? 1 : 0;
-                if (nb[u] != kInvalidEdge) { acc += to_fixed(xv[u], scale); ++st_g; }
+                if (slot_valid(nb[u])) { acc += to_fixed(xv[u], scale); ++st_g; }
             }
         }
         st_v += (light && gl == 0) ? 1 : 0;
@@ -370,10 +370,10 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
             for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? stream_col(d.cols + s + u * W) : kInvalidEdge;
             float xn[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) xn[u] = nb[u] != kInvalidEdge ? d.x[nb[u]] : 0.0f;
+            for (int u = 0; u < kSlotUnroll; ++u) xn[u] = slot_valid(nb[u]) ? d.x[nb[u]] : 0.0f;
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) {
-                if (nb[u] == kInvalidEdge) continue;
+                if (!slot_valid(nb[u])) continue;
                 const uint32_t o = ordered_bits(xn[u]);
                 const bool before = o < mine || (o == mine && nb[u] < v);
                 c += before ? -1 : 1;
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32
         uint32_t p = v;
         for (OffT s = beg; s < end; ++s) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge) continue;  // disabled slots keep their place in the sorted row
+            if (!slot_valid(nb)) continue;  // disabled slots keep their place in the sorted row
             if (nb >= v) break;                // no smaller neighbour left
             if (d.lab[nb] == lv) { p = nb; break; }
         }
@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(kBlock) k_union_sample(Dev<OffT> d, const uint
         const OffT beg = d.off[v], end = d.off[v + 1];
         if (end == beg) continue;
         const uint32_t nb = d.cols[beg + (OffT)(mix32(v) % (uint64_t)(end - beg))];
-        if (nb == kInvalidEdge || d.lab[nb] != lv) continue;
+        if (!slot_valid(nb) || d.lab[nb] != lv) continue;
         uint32_t hint = ld_relaxed(&d.parent[v]);
         uf_join(d.parent, &d.ctr->err, v, nb, hint);
     }
@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* i
         if (union_skip_row(d, k, v, lv, hint)) continue;
         for (OffT s = beg + gl; s < end; s += W) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge || nb == v) continue;
+            if (!slot_valid(nb) || nb == v) continue;
             if (!d.union_sampled && nb > v) break;   // each edge once, from its larger end
             if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
@@ -954,6 +954,18 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
     block_atomic_max(&d.ctr->max_csize_next, biggest);
 }
 
+// Certificate record of a vertex whose cluster is certified this round: the
+// round (+1), and bit 31 when the certified set (the component of root r,
+// acc_cnt[r] vertices) is not the whole cluster c swept this round, i.e. c
+// was cut or fell apart into components.  Certified vertices neither walk nor
+// recentre afterwards, so their potentials stay the ones this test saw.
+template <typename OffT>
+__device__ __forceinline__ void record_certificate(const Dev<OffT>& d, const ClusterTables& t, uint32_t v,
+                                                   uint32_t c, uint32_t r) {
+    const bool whole = d.cut_off[c] == kNoCut && d.acc_cnt[r] == t.size[c];
+    d.cert[v] = (d.ctr->rounds + 1u) | (whole ? 0u : 0x80000000u);
+}
+
 // Plain form: new labels and recentering (x -= cluster mean) over the
 // active list in vertex order, so labels, parents and potentials are read
 // and written in runs (k_apply then only compacts the sorted order).
@@ -972,6 +984,7 @@ __global__ void __launch_bounds__(kBlock) k_newlab(Dev<OffT> d, ClusterTables t,
         const int32_t nl = d.newlab[r];
         d.lab[v] = nl;
         if (nl >= 0) d.x[v] = __double2float_rn(__dsub_rn((double)d.x[v], d.avg[r]));
+        else record_certificate(d, t, v, c, r);
     }
 }
 
@@ -1021,6 +1034,8 @@ __global__ void __launch_bounds__(kBlock) k_apply(Dev<OffT> d, ClusterTables t, 
             d.x[v] = __double2float_rn(__dsub_rn((double)d.x[v], d.avg[r]));
             keepmask |= 1u << k;
             ++run;
+        } else {
+            record_certificate(d, t, v, c, r);
         }
     }
     uint64_t tile_total;
@@ -1114,11 +1129,11 @@ __global__ void __launch_bounds__(kBlock) k_ids_disable(Dev<OffT> d, const uint3
             for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * W < end ? stream_col(d.cols + s + u * W) : kInvalidEdge;
             int32_t ln[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) ln[u] = nb[u] != kInvalidEdge ? d.lab[nb[u]] : lv;
+            for (int u = 0; u < kSlotUnroll; ++u) ln[u] = slot_valid(nb[u]) ? d.lab[nb[u]] : lv;
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) {
-                if (nb[u] == kInvalidEdge) continue;
-                if (ln[u] != lv) d.cols[s + u * W] = kInvalidEdge;
+                if (!slot_valid(nb[u])) continue;
+                if (ln[u] != lv) d.cols[s + u * W] = nb[u] | kDisabledBit;
                 else ++deg;
             }
         }
@@ -1232,10 +1247,10 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
             for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? stream_col(d.cols + s + u * G) : kInvalidEdge;
             float xv[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) xv[u] = nb[u] != kInvalidEdge ? xt_in[nb[u]] : 0.0f;
+            for (int u = 0; u < kSlotUnroll; ++u) xv[u] = slot_valid(nb[u]) ? xt_in[nb[u]] : 0.0f;
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u)
-                if (nb[u] != kInvalidEdge) { acc += to_fixed(xv[u], scale); ++g; }
+                if (slot_valid(nb[u])) { acc += to_fixed(xv[u], scale); ++g; }
         }
         acc = group_sum<G, int64_t>(acc, sh);
         st_g += g;
@@ -1277,10 +1292,10 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
             for (int u = 0; u < kSlotUnroll; ++u) nb[u] = s + u * G < end ? stream_col(d.cols + s + u * G) : kInvalidEdge;
             float xn[kSlotUnroll];
 #pragma unroll
-            for (int u = 0; u < kSlotUnroll; ++u) xn[u] = nb[u] != kInvalidEdge ? d.x[nb[u]] : 0.0f;
+            for (int u = 0; u < kSlotUnroll; ++u) xn[u] = slot_valid(nb[u]) ? d.x[nb[u]] : 0.0f;
 #pragma unroll
             for (int u = 0; u < kSlotUnroll; ++u) {
-                if (nb[u] == kInvalidEdge) continue;
+                if (!slot_valid(nb[u])) continue;
                 const uint32_t o = ordered_bits(xn[u]);
                 c += (o < mine || (o == mine && nb[u] < v)) ? -1 : 1;
             }
@@ -1309,7 +1324,7 @@ __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
         if (union_skip_row(d, k, v, lv, hint)) continue;
         for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge || nb == v) continue;
+            if (!slot_valid(nb) || nb == v) continue;
             if (!d.union_sampled && nb > v) break;
             if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
@@ -1334,8 +1349,8 @@ __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt,
         uint32_t deg = 0;
         for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
-            if (nb == kInvalidEdge) continue;
-            if (d.lab[nb] != lv) d.cols[s] = kInvalidEdge;
+            if (!slot_valid(nb)) continue;
+            if (d.lab[nb] != lv) d.cols[s] = nb | kDisabledBit;
             else ++deg;
         }
         deg = group_sum<G, uint32_t>(deg, sh);

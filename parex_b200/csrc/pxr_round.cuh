@@ -79,6 +79,7 @@ struct Dev {
     uint32_t* acc_cnt;
     int32_t* newlab;      // by root vertex
     double* avg;          // by root vertex
+    uint32_t* cert;       // per vertex: certificate record (round + 1, bit 31: not the whole swept set)
     // per sorted position
     int32_t* pdif;
     uint32_t* pvol;

@@ -24,6 +24,11 @@ getNumClusters()            getNumClusters() (the reference returns 0; here the
 updateLabels(...)           updateLabels(...) (a no-op, as in cuda/devGraph.h:191-206)
 =========================  =====================================================
 
+Two members have no counterpart in the class: ``countCutEdges()`` recounts
+the cut edges of the final partition on the device (the count main.cpp:54-60
+makes on the host after getFinalPartition), and ``downloadCertificates()``
+returns the certificate record that parex_b200/certificate.py checks.
+
 Errors raise ``PxrError`` carrying the C status; the reference has no error
 reporting at all.
 """
@@ -210,6 +215,22 @@ class CudaDeviceManager:
     def downloadActiveEdgeMap(self) -> np.ndarray:
         out = np.zeros(2 * self.m, dtype=np.int32)
         self._call(self._L.pxr_active_edge_map, _ptr(out))
+        return out
+
+    def countCutEdges(self) -> int:
+        """Edges whose ends carry different final ids, recounted on the device
+        (pxr_count_cut_edges): what the reference's main.cpp computes on the
+        host after getFinalPartition (main.cpp:54-60)."""
+        out = C.c_uint64(0)
+        self._call(self._L.pxr_count_cut_edges, C.byref(out))
+        return int(out.value)
+
+    def downloadCertificates(self) -> np.ndarray:
+        """Certificate record per vertex (pxr_download_certificates): 0 while
+        active, else the certificate's round + 1, bit 31 set when the certified
+        set is not the whole set swept that round."""
+        out = np.zeros(self.n, dtype=np.uint32)
+        self._call(self._L.pxr_download_certificates, _ptr(out))
         return out
 
     def getNumClusters(self) -> int:
