@@ -57,7 +57,10 @@ typedef struct {
     uint32_t driver;         /* PXR_DRIVER_*                                              */
     uint32_t tune;           /* PXR_TUNE_* (row plan: lanes per row and row bins)          */
     uint32_t components;     /* PXR_COMPONENTS_* (union-find schedule of the cut stage)    */
-    uint32_t reserved[7];
+    uint32_t memory_cap_mib; /* device memory a handle may hold, in MiB (0: no cap); an
+                                initialisation that needs more fails with
+                                PXR_OUT_OF_MEMORY before any allocation is kept           */
+    uint32_t reserved[6];
 } pxr_config;
 
 /* Union-find schedule of the connected-components stage (no counterpart in
@@ -334,9 +337,10 @@ pxr_status pxr_phase_stats(pxr_handle* h, pxr_phase_stat* out, uint32_t cap, uin
  * Limit: n <= PXR_STATIC_SCRATCH_MAX_LABELS; larger n returns
  * PXR_INVALID_ARG (use pxr_final_partition).  The working memory is a fixed
  * ~1.1 MB array inside the library, held on every GPU that loads it until
- * the process exits.  The first call on each device looks up that array's
- * device address (cudaGetSymbolAddress) with the device current; make that
- * first call before any stream capture.  All calls share the array: calls
+ * the process exits.  Every call looks up that array's device address
+ * (cudaGetSymbolAddress) with the caller's device current, so a
+ * cudaDeviceReset between calls is harmless; the first call on a device also
+ * loads the library's kernels there, so make it before any stream capture.  All calls share the array: calls
  * whose work may overlap on the GPU race and must be ordered by the caller.
  * *num_clusters is -1 if a device-side bounded wait ran out. */
 #define PXR_STATIC_SCRATCH_MAX_LABELS 65536u
@@ -351,6 +355,16 @@ pxr_status pxr_set_potentials(pxr_handle* h, const double* x);
 pxr_status pxr_set_state(pxr_handle* h, const int32_t* labels, const uint32_t* act, uint32_t n_act,
                          const double* x, const uint32_t* internal_degrees, const uint32_t* cols,
                          uint32_t n_clusters, int32_t smallest_label, int full_components);
+
+/* Test hook with no counterpart in the reference: run the library's two
+ * bounded device-side waits - the decoupled look-back of the scans and the
+ * sort's tile-status wait - on a flag that nothing sets, with at most
+ * spin_limit polls (1 .. 2^20), on scratch memory of their own.  Both must
+ * give up, set their error bits and return; the call then reports
+ * PXR_DEVICE_FAULT the way a round that timed out does, *err_bits gets the
+ * bits, and the handle stays usable.  Nothing of the handle's state is
+ * touched. */
+pxr_status pxr_test_bounded_waits(pxr_handle* h, uint32_t spin_limit, uint32_t* err_bits);
 
 /* ---- graph construction on the device ------------------------------------
  * The CSR the reference builds on the host (readDynGraph +

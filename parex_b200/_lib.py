@@ -32,7 +32,7 @@ SYMBOLS = [
     "pxr_final_partition_static", "pxr_set_potentials", "pxr_set_state", "pxr_initialize_batched",
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
     "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
-    "pxr_rmat_edges", "pxr_sbm_edges", "pxr_initialize_batched_device",
+    "pxr_rmat_edges", "pxr_sbm_edges", "pxr_initialize_batched_device", "pxr_test_bounded_waits",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -41,7 +41,7 @@ class Config(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("sc_threshold", C.c_float), ("rw_threshold", C.c_float),
                 ("max_rounds", C.c_uint32), ("device", C.c_int32), ("division", C.c_uint32),
                 ("driver", C.c_uint32), ("tune", C.c_uint32), ("components", C.c_uint32),
-                ("reserved", C.c_uint32 * 7)]
+                ("memory_cap_mib", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 TUNE_AUTO, TUNE_HEURISTIC = 0, 1
@@ -162,6 +162,7 @@ def load() -> C.CDLL:
     L.pxr_download_labels.argtypes = [p, p]
     L.pxr_active_edge_map.argtypes = [p, p]
     L.pxr_count_cut_edges.argtypes = [p, C.POINTER(u64)]
+    L.pxr_test_bounded_waits.argtypes = [p, u32, C.POINTER(u32)]
     L.pxr_download_certificates.argtypes = [p, p]
     L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]
     L.pxr_get_stats.argtypes = [p, C.POINTER(Stats)]

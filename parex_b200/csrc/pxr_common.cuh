@@ -171,7 +171,7 @@ __device__ __forceinline__ void lookback_publish(LookbackState s, uint32_t tile,
 // (or tile 0) is reached.  Op must be commutative.  Every lane gets the result.
 template <class Op>
 __device__ __forceinline__ uint64_t lookback_exclusive(LookbackState s, uint32_t tile, uint32_t epoch,
-                                                       uint32_t* err) {
+                                                       uint32_t* err, uint32_t spin_limit = kSpinLimit) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t want = epoch & 0x3FFFFFFFu;
     uint64_t excl = Op::identity();
@@ -183,12 +183,12 @@ __device__ __forceinline__ uint64_t lookback_exclusive(LookbackState s, uint32_t
             uint32_t w = ld_acquire(&s.flags[t]);
             uint32_t spins = 0;
             while ((w >> 2) != want || (w & 3u) == 0u) {
-                if (++spins > kSpinLimit) { atomicOr(err, kErrLookback); w = (want << 2) | 2u; break; }
+                if (++spins > spin_limit) { atomicOr(err, kErrLookback); w = (want << 2) | 2u; break; }
                 __nanosleep(32);
                 w = ld_acquire(&s.flags[t]);
             }
             f = w & 3u;
-            if (spins <= kSpinLimit) v = (f == 2u) ? ld_relaxed64(&s.inc[t]) : ld_relaxed64(&s.agg[t]);
+            if (spins <= spin_limit) v = (f == 2u) ? ld_relaxed64(&s.inc[t]) : ld_relaxed64(&s.agg[t]);
         }
         const uint32_t inc_lanes = __ballot_sync(0xFFFFFFFFu, f == 2u);
         const uint32_t stop = inc_lanes ? (uint32_t)(__ffs(inc_lanes) - 1) : 31u;

@@ -84,6 +84,19 @@ __global__ void k_count_valid(const uint32_t* cols, uint64_t slots, unsigned lon
     if ((threadIdx.x & 31u) == 0 && c) atomicAdd(out, (unsigned long long)c);
 }
 
+// Test hook kernels: the look-back and the sort-status wait on flags that
+// nothing sets.  One warp each; scratch holds 2 look-back tiles and one
+// status word, all zero (epoch 0), and the waits ask for epoch 1.
+__global__ void k_test_lookback_wait(uint32_t* flags, uint64_t* agg, uint64_t* inc, uint32_t spin_limit,
+                                     uint32_t* err) {
+    LookbackState s{flags, agg, inc};
+    lookback_exclusive<Add64>(s, 1u, 1u, err, spin_limit);   // tile 0 never publishes
+}
+
+__global__ void k_test_sort_wait(const uint64_t* word, uint32_t spin_limit, uint32_t* err) {
+    if (threadIdx.x == 0) wait_sort_status(word, 1u, err, spin_limit);
+}
+
 // Cut edges of the partition given by the labels: CSR slots (both directions
 // of every edge) whose ends carry different labels, over the graph as
 // uploaded (a disabled slot still holds its neighbour under kDisabledBit).
@@ -408,6 +421,9 @@ template <typename T>
 cudaError_t dalloc(pxr_handle* h, T** p, size_t count) {
     void* q = nullptr;
     const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    // the handle's memory cap (pxr_config.memory_cap_mib) refuses like a full device
+    if (h->cfg.memory_cap_mib && h->bytes + bytes > ((size_t)h->cfg.memory_cap_mib << 20))
+        return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return e;
     h->allocs.push_back(q);
@@ -998,7 +1014,15 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     A(&h->d_num, 1); A(&h->d_valid, 1); A(&h->d_check, 4); A(&h->heavy, N); A(&h->wide, N);
     A(&h->probe_ctr, 1); A(&h->hist, 33);
 #undef A
-    if (e != cudaSuccess) { release(h); return cuda_fail(h, e, "cudaMalloc"); }
+    if (e != cudaSuccess) {
+        const size_t held = h->bytes;
+        release(h);
+        if (e == cudaErrorMemoryAllocation)
+            return fail(h, PXR_OUT_OF_MEMORY, "device memory exhausted after " + std::to_string(held >> 20) +
+                                                  " MiB" + (h->cfg.memory_cap_mib ? " (the handle's memory cap is " +
+                                                  std::to_string(h->cfg.memory_cap_mib) + " MiB)" : std::string()));
+        return cuda_fail(h, e, "cudaMalloc");
+    }
     h->sort.max_tiles = sort_tiles;
     h->sort.items_moved = &h->ctr->stat_sort_items;
     // look-back flags and sort status words carry epochs that only grow, so
@@ -1670,6 +1694,35 @@ pxr_status pxr_active_edge_map(pxr_handle* h, int32_t* out) {
     if (h->slots) PXR_CUDA(h, cudaMemcpyAsync(c.data(), h->cols, h->slots * 4, cudaMemcpyDeviceToHost, h->stream));
     PXR_CUDA(h, cudaStreamSynchronize(h->stream));
     for (uint64_t j = 0; j < h->slots; ++j) out[j] = slot_valid(c[j]) ? 1 : 0;
+    return PXR_OK;
+}
+
+pxr_status pxr_test_bounded_waits(pxr_handle* h, uint32_t spin_limit, uint32_t* err_bits) {
+    if (!h || !err_bits || spin_limit == 0 || spin_limit > kSpinLimit) return PXR_INVALID_ARG;
+    PXR_CUDA(h, cudaSetDevice(h->device));
+    // flags[2] | pad | agg[2] | inc[2] | status word | error word
+    unsigned char* scratch = nullptr;
+    constexpr size_t kBytes = 64;
+    PXR_CUDA(h, cudaMalloc(&scratch, kBytes));
+    uint32_t* flags = reinterpret_cast<uint32_t*>(scratch);
+    uint64_t* agg = reinterpret_cast<uint64_t*>(scratch + 8);
+    uint64_t* inc = reinterpret_cast<uint64_t*>(scratch + 24);
+    uint64_t* word = reinterpret_cast<uint64_t*>(scratch + 40);
+    uint32_t* err = reinterpret_cast<uint32_t*>(scratch + 48);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, kBytes, h->stream);
+    if (e == cudaSuccess) {
+        k_test_lookback_wait<<<1, 32, 0, h->stream>>>(flags, agg, inc, spin_limit, err);
+        k_test_sort_wait<<<1, 32, 0, h->stream>>>(word, spin_limit, err);
+        h->launches += 2;
+        e = cudaGetLastError();
+    }
+    uint32_t bits = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, err, 4, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(scratch);
+    if (e != cudaSuccess) return cuda_fail(h, e, "bounded-wait test");
+    *err_bits = bits;
+    if (bits) return fail(h, PXR_DEVICE_FAULT, "device-side bounded wait ran out (bits " + std::to_string(bits) + ")");
     return PXR_OK;
 }
 

@@ -112,6 +112,23 @@ __device__ __forceinline__ uint64_t sort_status_word(uint32_t epoch, uint32_t fl
     return ((uint64_t)((epoch << 2) | flag) << 32) | cnt;
 }
 
+// A predecessor tile's status word for this epoch, polled at most spin_limit
+// times; when it never arrives the error bit is set and the stale word is
+// returned.  Tile ids are taken in launch order, so a predecessor is always
+// resident or done and the limit (about a second) is reached only if the
+// protocol itself is broken; the host then reports PXR_DEVICE_FAULT.
+__device__ __forceinline__ uint64_t wait_sort_status(const uint64_t* word, uint32_t epoch, uint32_t* err,
+                                                     uint32_t spin_limit = kSpinLimit) {
+    uint64_t w = ld_relaxed64(word);
+    uint32_t spins = 0;
+    while ((uint32_t)(w >> 34) != (epoch & 0x3FFFFFFFu) || ((w >> 32) & 3u) == 0u) {
+        if (++spins > spin_limit) { atomicOr(err, kErrSortTiles); break; }
+        __nanosleep(32);
+        w = ld_relaxed64(word);
+    }
+    return w;
+}
+
 template <typename K>
 #ifndef PXR_SORT_MIN_BLOCKS
 #define PXR_SORT_MIN_BLOCKS 2
@@ -193,14 +210,7 @@ __global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_k
     st_relaxed64(st, sort_status_word(epoch, 1u, tile_cnt));
     uint32_t excl = 0;
     for (int32_t t = (int32_t)tile - 1; t >= 0; --t) {
-        const uint64_t* other = s.status + (size_t)t * kRadix + d;
-        uint64_t w = ld_relaxed64(other);
-        uint32_t spins = 0;
-        while ((uint32_t)(w >> 34) != (epoch & 0x3FFFFFFFu) || ((w >> 32) & 3u) == 0u) {
-            if (++spins > kSpinLimit) { atomicOr(err, kErrSortTiles); break; }
-            __nanosleep(32);
-            w = ld_relaxed64(other);
-        }
+        const uint64_t w = wait_sort_status(s.status + (size_t)t * kRadix + d, epoch, err);
         excl += (uint32_t)w;
         if (((w >> 32) & 3u) == 2u) break;
     }

@@ -13,17 +13,16 @@
 // The scratch array (g_scratch) is a file-scope __device__ array: every GPU
 // that loads the library holds it (about 1.1 MB) until the process exits.
 // Host code cannot use g_scratch's name as an address - in host code that
-// name is only a stand-in - so the first call on each device resolves the
-// real device address with cudaGetSymbolAddress while that device is current,
-// and later calls on that device reuse it.  The first call on a device should
-// therefore be made before any stream capture begins.
+// name is only a stand-in - so every call resolves the real device address
+// with cudaGetSymbolAddress while the caller's device is current (nothing is
+// cached, so a cudaDeviceReset between calls is harmless).  The first call
+// on a device also loads the library's kernels there and should therefore be
+// made before any stream capture begins.
 //
 // All calls share the one array and it keeps the previous call's contents,
 // so every call first clears the parts that must start at zero.  Calls whose
 // work overlaps on the GPU (different streams, no ordering between them)
 // race on the array and must be avoided.
-#include <mutex>
-
 #include "pxr_kernels.cuh"
 
 namespace pxr {
@@ -124,34 +123,17 @@ __global__ void __launch_bounds__(kBlock) k_static_rank(unsigned char* base, int
 
 __global__ void k_static_zero(int32_t* num_out) { *num_out = 0; }
 
-// Per-device address of g_scratch, resolved on the first call on each device.
-struct DeviceSlot {
-    unsigned char* base = nullptr;
-    bool sort_ready = false;
-};
-constexpr int kMaxDevices = 64;
-DeviceSlot g_slots[kMaxDevices];
-std::mutex g_lock;
-
+// Device address of g_scratch on the current device, looked up on every call
+// with that device current, and the sort kernels' shared-memory attribute
+// set again: both are cheap, and nothing cached can outlive a
+// cudaDeviceReset in the caller's process.
 cudaError_t scratch_for_current_device(unsigned char** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> guard(g_lock);
-    DeviceSlot& slot = g_slots[dev];
-    if (!slot.base) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess) return e;
-        slot.base = static_cast<unsigned char*>(p);
-    }
-    if (!slot.sort_ready) {
-        e = radix_sort_prepare<uint32_t>();
-        if (e != cudaSuccess) return e;
-        slot.sort_ready = true;
-    }
-    *out = slot.base;
+    e = radix_sort_prepare<uint32_t>();
+    if (e != cudaSuccess) return e;
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 

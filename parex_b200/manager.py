@@ -67,7 +67,7 @@ class CudaDeviceManager:
     def __init__(self, seed: int = 6582, sc_threshold: float = 0.3, rw_threshold: float = 1e-4,
                  max_rounds: int = 200000, device: int = 0, division: int = _lib.DIV_IEEE,
                  driver: int = _lib.DRIVER_GRAPH, tune: int = _lib.TUNE_AUTO,
-                 components: int = _lib.COMPONENTS_AUTO):
+                 components: int = _lib.COMPONENTS_AUTO, memory_cap_mib: int = 0):
         L = _lib.load()
         cfg = _lib.Config()
         L.pxr_config_default(C.byref(cfg))
@@ -80,6 +80,7 @@ class CudaDeviceManager:
         cfg.driver = driver
         cfg.tune = tune
         cfg.components = components
+        cfg.memory_cap_mib = memory_cap_mib
         self._h = C.c_void_p()
         _lib.check(None, L.pxr_create(C.byref(cfg), C.byref(self._h)))
         self._L = L

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_sizes_match_header():
-    # pxr_config: 7 x 4-byte fields + reserved[9]
+    # pxr_config: 10 four-byte fields + reserved[6]
     assert C.sizeof(_lib.Config) == 64
     assert C.sizeof(_lib.SweepCut) == 12      # SweepCutData
     assert C.sizeof(_lib.NodeData) == 16      # NodeData
