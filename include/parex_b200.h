@@ -96,6 +96,21 @@ typedef struct {
     float walk_us;           /* walk-step time of the chosen plan when tuned (microseconds)  */
 } pxr_row_plan;
 
+/* Sort plan of the sweep's global radix sort (no counterpart in the
+ * reference, which calls CUB's SortPairs): keys per thread of a tile (16, 12
+ * or 8; tiles of 256 x items) and the CTAs per SM the pass kernel's register
+ * budget is sized for (2, 3 or 4), as plan 0, 1 or 2.  Digits are 8 bits
+ * wide; passes whose digit is constant over the keys are skipped.  Every plan
+ * gives the same order, item for item. */
+typedef struct {
+    uint32_t plan;           /* 0, 1 or 2                                                    */
+    uint32_t items_per_thread;
+    uint32_t ctas_per_sm;
+    uint32_t source;         /* 0 default, 1 tuned now, 2 tuned earlier (cache), 3 forced      */
+    uint32_t candidates;     /* plans timed by the last tuning                               */
+    float sort_us[3];        /* time of one sort of the first round's keys under each plan   */
+} pxr_sort_plan;
+
 /* One sweep cut per active cluster: SweepCutData, lib/core/definitions.h:57-61. */
 typedef struct { int32_t label; float sparsity; uint32_t offset; } pxr_sweep_cut;
 
@@ -244,6 +259,16 @@ pxr_status pxr_get_row_plan(pxr_handle* h, pxr_row_plan* out);
  * ignored) for this and later initialisations; NULL returns to cfg.tune.
  * Applied at once when a graph is loaded. */
 pxr_status pxr_set_row_plan(pxr_handle* h, const pxr_row_plan* plan);
+
+/* The sweep sort's plan in use (pxr_sort_plan).  With PXR_TUNE_AUTO the
+ * library times the global sort of the first round's keys (every active
+ * vertex, cluster 0) under each plan when a graph of at least 2^16 vertices
+ * is loaded and keeps the fastest; choices are cached per vertex count.  No
+ * counterpart in the reference. */
+pxr_status pxr_get_sort_plan(pxr_handle* h, pxr_sort_plan* out);
+/* Force a sort plan (plan is read) from the next round on; NULL returns to
+ * cfg.tune from the next initialisation. */
+pxr_status pxr_set_sort_plan(pxr_handle* h, const pxr_sort_plan* plan);
 
 /* pxr_initialize_batched with the CSR in device memory (offsets 64-bit when
  * offsets_are_64bit, else 32-bit); instance_start stays a host array. */

@@ -33,8 +33,14 @@ SYMBOLS = [
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
     "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
     "pxr_rmat_edges", "pxr_sbm_edges", "pxr_initialize_batched_device", "pxr_test_bounded_waits",
+    "pxr_get_sort_plan", "pxr_set_sort_plan",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
+
+
+class SortPlan(C.Structure):
+    _fields_ = [("plan", C.c_uint32), ("items_per_thread", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("source", C.c_uint32), ("candidates", C.c_uint32), ("sort_us", C.c_float * 3)]
 
 
 class Config(C.Structure):
@@ -163,6 +169,8 @@ def load() -> C.CDLL:
     L.pxr_active_edge_map.argtypes = [p, p]
     L.pxr_count_cut_edges.argtypes = [p, C.POINTER(u64)]
     L.pxr_test_bounded_waits.argtypes = [p, u32, C.POINTER(u32)]
+    L.pxr_get_sort_plan.argtypes = [p, C.POINTER(SortPlan)]
+    L.pxr_set_sort_plan.argtypes = [p, C.POINTER(SortPlan)]
     L.pxr_download_certificates.argtypes = [p, p]
     L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]
     L.pxr_get_stats.argtypes = [p, C.POINTER(Stats)]

@@ -365,6 +365,8 @@ struct pxr_handle {
     RoundCtr* probe_ctr = nullptr;    // scratch counters for the tuner's timed walk steps
     bool plan_forced = false;
     pxr_row_plan plan_info{};         // last plan chosen (pxr_get_row_plan)
+    bool sort_forced = false;
+    pxr_sort_plan sort_info{0, 16, 2, 0, 0, {0.0f, 0.0f, 0.0f}};   // sweep sort plan (pxr_get_sort_plan)
     uint32_t light_max = kLightRow;   // row bins (see k_bin_rows)
     uint32_t wide_max = kWideRow;
     uint32_t* wide = nullptr;
@@ -717,7 +719,9 @@ cudaError_t op_sweep(pxr_handle* h) {
     }
     phase(h, kPhSort, (run_gsort ? kGsortLaunches : 0) + (run_chunk ? 1 : 0), [&] {
         if (run_gsort)
-            e = if_region(h, c_gsort, [&](cudaStream_t st) { return radix_sort<uint64_t>(b, h->sort, &h->ctr->err, st, 64); });
+            e = if_region(h, c_gsort, [&](cudaStream_t st) {
+                return radix_sort<uint64_t>(b, h->sort, &h->ctr->err, st, 64, (int)h->sort_info.plan);
+            });
         // the chunked sort writes buffer 0, which round preparation selects
         if (e == cudaSuccess && run_chunk)
             e = if_region(h, c_chunk, [&](cudaStream_t st) {
@@ -985,7 +989,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     const size_t N = std::max<uint32_t>(n, 1);
     // look-back state per site, sized for the smallest tile (k_relabel's)
     const uint32_t scan_tiles = (uint32_t)((N + kRelabelTile - 1) / kRelabelTile) + 1;
-    const uint32_t sort_tiles = (uint32_t)((N + kSortTile - 1) / kSortTile) + 1;
+    const uint32_t sort_tiles = (uint32_t)((N + kSortMinTile - 1) / kSortMinTile) + 1;   // any sort plan's tiles
     cudaError_t e = cudaSuccess;
 #define A(ptr, cnt) if (e == cudaSuccess) e = dalloc(h, ptr, cnt)
     A(reinterpret_cast<OffT**>(&h->off), (size_t)n + 1);
@@ -1229,6 +1233,95 @@ pxr_status choose_row_plan(pxr_handle* h, bool reuse, uint32_t nb_bits) {
     return PXR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Sort-plan autotuner: time the global sort of the first round's keys (label
+// 0, the ordered bits of every vertex's potential, values the vertex ids) under
+// each plan of kSortPlans and keep the fastest.  The keys live in the sort
+// buffers, which hold nothing before the first round.  Cached per vertex
+// count for the life of the process.
+
+std::map<uint64_t, std::pair<uint32_t, std::array<float, 3>>> g_sort_cache;
+constexpr uint32_t kSortTuneMinVertices = 1u << 16;
+
+__global__ void k_tune_sort_keys(const float* x, uint32_t n, uint64_t* keys, uint32_t* vals) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        keys[v] = ordered_bits(x[v]);
+        vals[v] = v;
+    }
+}
+
+pxr_status tune_sort_plan(pxr_handle* h, uint32_t* best, std::array<float, 3>* us) {
+    cudaStream_t s = h->stream;
+    const uint32_t n = h->n;
+    SortBuffers<uint64_t> b{};
+    b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
+    b.vals[0] = h->vals[0]; b.vals[1] = h->vals[1];
+    b.count = h->d_n;
+    b.end_bit = h->fp_end_bit;   // 32 bits: the potential part of a cluster-0 key
+    b.capacity = n;
+    SortState st = h->sort;
+    st.items_moved = nullptr;    // the probe sorts stay out of the traffic counters
+    cudaEvent_t e0 = take_event(h), e1 = take_event(h);
+    constexpr int kReps = 3;
+    float best_ms = 0.0f;
+    for (int p = 0; p < kSortPlanCount; ++p) {
+        float total = 0.0f;
+        for (int r = 0; r <= kReps; ++r) {   // the first run warms up
+            k_tune_sort_keys<<<grid_for(n), kBlock, 0, s>>>(h->x, n, h->keys[0], h->vals[0]);
+            cudaEventRecord(e0, s);
+            PXR_CUDA(h, radix_sort<uint64_t>(b, st, &h->ctr->err, s, 32, p));
+            cudaEventRecord(e1, s);
+            PXR_CUDA(h, cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            PXR_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+            if (r > 0) total += ms;
+            h->launches += 1 + 2 + 4;
+        }
+        (*us)[p] = total * 1000.0f / kReps;
+        if (p == 0 || total < best_ms) { best_ms = total; *best = (uint32_t)p; }
+    }
+    h->event_pool.push_back(e0);
+    h->event_pool.push_back(e1);
+    return PXR_OK;
+}
+
+// The sweep sort's plan for the graph just uploaded: forced, cached, tuned or
+// the default.  Drops captured graphs when the plan changed.
+pxr_status choose_sort_plan(pxr_handle* h) {
+    const uint32_t old = h->sort_info.plan;
+    uint32_t plan = 0, source = 0, tried = 0;
+    std::array<float, 3> us{0.0f, 0.0f, 0.0f};
+    if (h->sort_forced) {
+        plan = h->sort_info.plan;
+        source = 3;
+    } else if (h->cfg.tune == PXR_TUNE_AUTO && h->n >= kSortTuneMinVertices) {
+        bool hit = false;
+        {
+            std::lock_guard<std::mutex> lk(g_plan_mu);
+            auto it = g_sort_cache.find(h->n);
+            if (it != g_sort_cache.end()) { plan = it->second.first; us = it->second.second; hit = true; }
+        }
+        if (hit) {
+            source = 2;
+        } else {
+            pxr_status st = tune_sort_plan(h, &plan, &us);
+            if (st != PXR_OK) return st;
+            source = 1;
+            tried = kSortPlanCount;
+            std::lock_guard<std::mutex> lk(g_plan_mu);
+            g_sort_cache[h->n] = {plan, us};
+        }
+    }
+    if (plan != old) drop_graphs(h);
+    h->sort_info.plan = plan;
+    h->sort_info.items_per_thread = (uint32_t)kSortPlans[plan].items;
+    h->sort_info.ctas_per_sm = (uint32_t)kSortPlans[plan].ctas;
+    h->sort_info.source = source;
+    if (source != 3) h->sort_info.candidates = tried;
+    for (int p = 0; p < 3; ++p) h->sort_info.sort_us[p] = us[p];
+    return PXR_OK;
+}
+
 // offsets/cols: host pointers (kind = cudaMemcpyHostToDevice) or device pointers
 template <typename OffT>
 pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* offsets, const uint32_t* cols,
@@ -1288,6 +1381,7 @@ pxr_status initialize_impl(pxr_handle* h, uint32_t n, uint64_t m, const OffT* of
     pxr_status st = setup_tables_initial(h);
     if (st == PXR_OK) st = reset_schedule_state(h);
     if (st == PXR_OK) st = choose_row_plan<OffT>(h, reuse, nb_bits);
+    if (st == PXR_OK) st = choose_sort_plan(h);
     if (st != PXR_OK) return st;
     PXR_CUDA(h, cudaGetLastError());
     if (batched) return PXR_OK;   // batch_setup completes the state
@@ -1951,6 +2045,28 @@ pxr_status pxr_read_cluster_records(pxr_handle* h, pxr_cluster_record* out, uint
 pxr_status pxr_get_row_plan(pxr_handle* h, pxr_row_plan* out) {
     if (!h || !out) return PXR_INVALID_ARG;
     *out = h->plan_info;
+    return PXR_OK;
+}
+
+pxr_status pxr_get_sort_plan(pxr_handle* h, pxr_sort_plan* out) {
+    if (!h || !out) return PXR_INVALID_ARG;
+    *out = h->sort_info;
+    return PXR_OK;
+}
+
+pxr_status pxr_set_sort_plan(pxr_handle* h, const pxr_sort_plan* plan) {
+    if (!h) return PXR_INVALID_ARG;
+    if (plan) {
+        if (plan->plan >= (uint32_t)kSortPlanCount) return fail(h, PXR_INVALID_ARG, "sort plan must be 0, 1 or 2");
+        if (plan->plan != h->sort_info.plan) drop_graphs(h);
+        h->sort_forced = true;
+        h->sort_info.plan = plan->plan;
+        h->sort_info.items_per_thread = (uint32_t)kSortPlans[plan->plan].items;
+        h->sort_info.ctas_per_sm = (uint32_t)kSortPlans[plan->plan].ctas;
+        h->sort_info.source = 3;
+    } else {
+        h->sort_forced = false;   // the tuned or default plan returns with the next graph
+    }
     return PXR_OK;
 }
 

@@ -129,12 +129,17 @@ __device__ __forceinline__ uint64_t wait_sort_status(const uint64_t* word, uint3
     return w;
 }
 
-template <typename K>
 #ifndef PXR_SORT_MIN_BLOCKS
 #define PXR_SORT_MIN_BLOCKS 2
 #endif
-__global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_kernel(SortBuffers<K> b, SortState s, int pass,
-                                                                 uint32_t* err) {
+// One digit pass.  ITEMS keys per thread (tile = 256 ITEMS) and the CTAs per
+// SM the register budget is sized for (MINB) are the sort plan's two axes
+// (pxr_sort_plan); every plan gives the same output, item for item.
+template <typename K, int ITEMS = kSortItems, int MINB = PXR_SORT_MIN_BLOCKS>
+__global__ void __launch_bounds__(kSortThreads, MINB) sort_pass_kernel(SortBuffers<K> b, SortState s, int pass,
+                                                                       uint32_t* err) {
+    constexpr int kSortItems = ITEMS;
+    constexpr int kSortTile = kSortThreads * ITEMS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K* skeys = reinterpret_cast<K*>(smem_raw);
     uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);
@@ -242,31 +247,58 @@ __global__ void __launch_bounds__(kSortThreads, PXR_SORT_MIN_BLOCKS) sort_pass_k
     }
 }
 
-template <typename K>
+template <typename K, int ITEMS = kSortItems>
 constexpr size_t sort_pass_smem() {
-    return sizeof(K) * kSortTile + sizeof(uint32_t) * kSortTile + sizeof(uint32_t) * (kSortThreads / 32) * kRadix;
+    return (sizeof(K) + sizeof(uint32_t)) * kSortThreads * ITEMS + sizeof(uint32_t) * (kSortThreads / 32) * kRadix;
 }
 
-// Launch a full sort on `stream`.  After it, s.pass_info[kMaxPasses] on the
-// device names the buffer (0/1) holding the sorted keys and values.
+// Sort plans (items per thread, CTAs per SM) the tuner chooses from; plan 0
+// is the default.  The smallest tile sets how many tile status words a sort
+// may need (kSortMinTile).
+struct SortPlanEntry { int items, ctas; };
+constexpr SortPlanEntry kSortPlans[3] = {{16, 2}, {12, 3}, {8, 4}};
+constexpr int kSortPlanCount = 3;
+constexpr int kSortMinTile = kSortThreads * 8;
+
+template <typename K, int ITEMS, int MINB>
+inline void launch_sort_passes(const SortBuffers<K>& b, const SortState& s, uint32_t* err, cudaStream_t stream,
+                               int npasses) {
+    const uint32_t tiles = (b.capacity + kSortThreads * ITEMS - 1) / (kSortThreads * ITEMS);
+    for (int p = 0; p < npasses; ++p)
+        sort_pass_kernel<K, ITEMS, MINB><<<tiles, kSortThreads, sort_pass_smem<K, ITEMS>(), stream>>>(b, s, p, err);
+}
+
+// Launch a full sort on `stream` with sort plan `plan` (index into
+// kSortPlans).  After it, s.pass_info[kMaxPasses] on the device names the
+// buffer (0/1) holding the sorted keys and values.
 template <typename K>
 inline cudaError_t radix_sort(const SortBuffers<K>& b, const SortState& s, uint32_t* err, cudaStream_t stream,
-                              int max_end_bit) {
+                              int max_end_bit, int plan = 0) {
     if (b.capacity == 0) return cudaSuccess;
     const uint32_t tiles = (b.capacity + kSortTile - 1) / kSortTile;
     const uint32_t hgrid = min(tiles * 4u, 148u * 8u);
     sort_histogram_kernel<K><<<hgrid, kSortThreads, 0, stream>>>(b, s);
     sort_plan_kernel<K><<<1, kRadix, 0, stream>>>(b, s);
     const int npasses = (max_end_bit + 7) / 8;
-    for (int p = 0; p < npasses; ++p)
-        sort_pass_kernel<K><<<tiles, kSortThreads, sort_pass_smem<K>(), stream>>>(b, s, p, err);
+    switch (plan) {
+        case 1: launch_sort_passes<K, 12, 3>(b, s, err, stream, npasses); break;
+        case 2: launch_sort_passes<K, 8, 4>(b, s, err, stream, npasses); break;
+        default: launch_sort_passes<K, 16, PXR_SORT_MIN_BLOCKS>(b, s, err, stream, npasses); break;
+    }
     return cudaGetLastError();
 }
 
 template <typename K>
 inline cudaError_t radix_sort_prepare() {
-    return cudaFuncSetAttribute(sort_pass_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sort_pass_smem<K>());
+    cudaError_t e = cudaFuncSetAttribute(sort_pass_kernel<K, 16, PXR_SORT_MIN_BLOCKS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_pass_smem<K, 16>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sort_pass_kernel<K, 12, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sort_pass_smem<K, 12>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sort_pass_kernel<K, 8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sort_pass_smem<K, 8>());
+    return e;
 }
 
 }  // namespace pxr

@@ -301,6 +301,23 @@ class CudaDeviceManager:
         rp = _lib.RowPlan(lanes_per_row, light_max, wide_max)
         self._call(self._L.pxr_set_row_plan, C.byref(rp))
 
+    def sort_plan(self) -> dict:
+        """The sweep sort's plan in use (pxr_get_sort_plan)."""
+        sp = _lib.SortPlan()
+        self._call(self._L.pxr_get_sort_plan, C.byref(sp))
+        out = {f: getattr(sp, f) for f, _ in _lib.SortPlan._fields_ if f != "sort_us"}
+        out["sort_us"] = [float(v) for v in sp.sort_us]
+        return out
+
+    def set_sort_plan(self, plan: int | None = None) -> None:
+        """Force sort plan 0, 1 or 2; with no argument return to the configured tuning."""
+        if plan is None:
+            self._call(self._L.pxr_set_sort_plan, None)
+            return
+        sp = _lib.SortPlan()
+        sp.plan = plan
+        self._call(self._L.pxr_set_sort_plan, C.byref(sp))
+
     def set_stream(self, stream_ptr: int | None) -> None:
         self._call(self._L.pxr_set_stream, C.c_void_p(stream_ptr) if stream_ptr else None)
 

@@ -109,3 +109,45 @@ def test_components_schedules_agree(name):
         np.testing.assert_array_equal(ids, out[0][0])
         assert cut == out[0][1]
         np.testing.assert_array_equal(lab, out[0][2])
+
+
+# ---------------------------------------------------------------------------
+# sort plans (pxr_get_sort_plan / pxr_set_sort_plan): keys per thread and CTAs
+# per SM of the sweep's radix sort change speed only
+
+
+@pytest.mark.parametrize("name", ["rmat13", "grid12"])
+@pytest.mark.parametrize("driver", [P.DRIVER_GRAPH, P.DRIVER_STREAM])
+def test_results_do_not_depend_on_the_sort_plan(name, driver):
+    g = GRAPHS[name]()
+    runs = []
+    for plan in (0, 1, 2):
+        dm = P.CudaDeviceManager(driver=driver)
+        dm.set_sort_plan(plan)
+        dm.initialize(g)
+        dm.expanderDecomposition()
+        sp = dm.sort_plan()
+        assert sp["plan"] == plan and sp["source"] == 3
+        assert (sp["items_per_thread"], sp["ctas_per_sm"]) == [(16, 2), (12, 3), (8, 4)][plan]
+        runs.append((dm.getFinalPartition().clusterIds, dm.downloadLabels(), dm.readRandomWalkValues()))
+    for ids, labels, x in runs[1:]:
+        np.testing.assert_array_equal(ids, runs[0][0])
+        np.testing.assert_array_equal(labels, runs[0][1])
+        np.testing.assert_array_equal(x.view(np.uint32), runs[0][2].view(np.uint32))
+
+
+def test_sort_plan_is_tuned_and_cached():
+    g = G.grid3d(48)     # 110,592 vertices: above the tuning threshold
+    a = P.CudaDeviceManager()
+    a.initialize(g)
+    first = a.sort_plan()
+    assert first["source"] in (1, 2) and first["plan"] in (0, 1, 2)
+    assert all(t > 0 for t in first["sort_us"])
+    assert first["plan"] == int(np.argmin(first["sort_us"]))
+    b = P.CudaDeviceManager()
+    b.initialize(g)
+    assert b.sort_plan()["source"] == 2 and b.sort_plan()["plan"] == first["plan"]
+    # the probe sorts are not counted as sweep traffic
+    assert b.stats()["sort_items"] == 0
+    with pytest.raises(Exception):
+        b.set_sort_plan(3)
