@@ -110,6 +110,47 @@ def collect_trace(graph, seed: int, sc: float = 0.3, rw: float = 1e-4, device: i
     return np.concatenate(out) if out else np.zeros(0, dtype=_lib.RECORD_DTYPE)
 
 
+LIGHT_DTYPE = np.dtype([("root", "<u4"), ("size", "<u4"), ("origin", "<u4"), ("round", "<u4")])
+
+
+def collect_samples(graph, seed: int, sc: float = 0.3, rw: float = 1e-4, device: int = 0,
+                    max_rounds: int = 10000, per_round: int = 20000, sample_seed: int = 0):
+    """Training samples of one plain decomposition, for graphs whose full
+    trace would not fit in host memory (the 128^3 grid has up to ~800 k
+    clusters per round): the identity (root, size), origin and round of every
+    record are kept, so targets follow every vertex set across rounds; the
+    features only of at most ``per_round`` swept clusters per round, drawn
+    uniformly.  Returns (features, targets) as dataset() does."""
+    dm = CudaDeviceManager(seed=seed, sc_threshold=sc, rw_threshold=rw, device=device, driver=_lib.DRIVER_STREAM)
+    dm.set_schedule(_lib.SCHEDULE_PLAIN, trace=True)
+    dm.initialize(graph)
+    rng = np.random.default_rng(sample_seed)
+    light, feats, picked = [], [], []
+    base = 0
+    for _ in range(max_rounds):
+        if dm.getNumClusters() == 0:
+            break
+        dm.iterateRandomWalk()
+        dm.computeSweepCuts()
+        dm.cutClusters()
+        rec = dm.cluster_records()
+        lr = np.zeros(rec.shape[0], dtype=LIGHT_DTYPE)
+        for f in LIGHT_DTYPE.names:
+            lr[f] = rec[f]
+        light.append(lr)
+        swept = np.nonzero(rec["origin"] == ORIGIN_SWEPT)[0]
+        if swept.size > per_round:
+            swept = np.sort(rng.choice(swept, per_round, replace=False))
+        feats.append(rec["features"][swept].astype(np.float32))
+        picked.append(base + swept)
+        base += rec.shape[0]
+    dm.close()
+    if not light:
+        return np.zeros((0, F), np.float32), np.zeros(0, np.float32)
+    t = trace_targets(np.concatenate(light))[np.concatenate(picked)]
+    return np.concatenate(feats), np.log2(1.0 + np.minimum(t, 255)).astype(np.float32)
+
+
 def trace_targets(rec: np.ndarray) -> np.ndarray:
     """Safe skips of every record: the number of following rounds in which the
     same vertex set (same root and size) was swept without being cut or
@@ -252,8 +293,11 @@ def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, ma
         times.append(dm.stats()["last_decompose_ms"])
     fp = dm.getFinalPartition()
     st = dm.stats()
-    return {"ms": min(times), "rounds": rounds, "clusters": fp.numClusters,
-            "cut_edges": cut_edges(graph, fp.clusterIds), "device_cut_edges": dm.getNumCutEdges(),
+    from . import certificate
+    cert = certificate.check(graph.offsets, graph.cols, fp.clusterIds, dm.readRandomWalkValues(),
+                             dm.downloadCertificates(), sc, rw, device=f"cuda:{device}")
+    return {"ms": min(times), "rounds": rounds, "clusters": fp.numClusters, "certified": cert["ok"],
+            "cut_edges": dm.countCutEdges(), "device_cut_edges": dm.getNumCutEdges(),
             "swept_items": st["swept_items"], "skipped_sweeps": st["skipped_sweeps"],
             "false_stops": st["false_stops"], "ids": fp.clusterIds}
 
@@ -277,16 +321,27 @@ def compare(graph, model: Model, seed: int = 6582, safety: float = 0.25, max_ski
     return res
 
 
+def _rmat_device_built(scale: int, seed: int):
+    from . import gpu_build as B
+    off, cols, _, _ = B.rmat(scale, 16, seed=seed)
+    return B.to_host(off, cols, f"rmat_{scale}_{seed}")
+
+
+# Traces of the plain method on the benchmark's first three configurations,
+# at seeds disjoint from every evaluation: (name, graph from seed, walk seed
+# from seed, seeds).  Planted partition n=16384 (graph seeds 11-13), the 128^3
+# grid (walk seeds 1 and 2; the evaluation walks from 6582) and R-MAT scale 22
+# (graph seeds 2 and 3; evaluations use seeds 1, 101 and 202).
 TRAIN_GRAPHS = [
-    ("sbm16k", lambda s: G.sbm_graph(16384, 16, 12.0, 0.5, s), [11, 12, 13]),
-    ("grid48", lambda s: G.grid3d(48), [21, 22]),
-    ("grid64", lambda s: G.grid3d(64), [23]),
-    ("rmat16", lambda s: G.rmat(16, 16, seed=s), [31, 32]),
+    ("sbm16k", lambda s: G.sbm_graph(16384, 16, 12.0, 0.5, s), lambda s: 6582, [11, 12, 13]),
+    ("grid128", lambda s: G.grid3d(128), lambda s: s, [1, 2]),
+    ("rmat22", lambda s: _rmat_device_built(22, s), lambda s: 6582, [2, 3]),
 ]
 EVAL_GRAPHS = [
     ("sbm16k_6582", lambda: G.sbm_graph(16384, 16, 12.0, 0.5, 6582), 6582),
     ("grid128", lambda: G.grid3d(128), 6582),
-    ("rmat18", lambda: G.rmat(18, 16, seed=1), 6582),
+    ("rmat18_seed101", lambda: G.rmat(18, 16, seed=101), 6582),
+    ("rmat22_seed1", lambda: _rmat_device_built(22, 1), 6582),
 ]
 
 
@@ -303,6 +358,7 @@ def main(argv=None) -> int:
     t.add_argument("--safety", type=float, nargs="*", default=[0.25])
     t.add_argument("--max-skip", type=int, default=16)
     t.add_argument("--report", default=None)
+    t.add_argument("--per-round", type=int, default=20000, help="swept clusters sampled per round of a trace")
     e = sub.add_parser("eval")
     e.add_argument("--model", default=DEFAULT_MODEL)
     e.add_argument("--safety", type=float, nargs="*", default=[0.25])
@@ -312,17 +368,19 @@ def main(argv=None) -> int:
     log = lambda s: print(s, file=sys.stderr, flush=True)
     report = {}
     if args.cmd == "train":
-        traces = []
-        for name, make, seeds in TRAIN_GRAPHS:
+        xs, ts = [], []
+        for name, make, walk_seed, seeds in TRAIN_GRAPHS:
             for s in seeds:
                 t0 = time.perf_counter()
-                rec = collect_trace(make(s), seed=s)
-                traces.append(rec)
-                log(f"trace {name} seed {s}: {rec.shape[0]} records, {time.perf_counter() - t0:.1f} s")
-        X, T = dataset(traces)
+                X1, T1 = collect_samples(make(s), seed=walk_seed(s), per_round=args.per_round)
+                xs.append(X1)
+                ts.append(T1)
+                log(f"trace {name} seed {s}: {X1.shape[0]} samples, {time.perf_counter() - t0:.1f} s")
+        X, T = np.concatenate(xs), np.concatenate(ts)
         log(f"dataset: {X.shape[0]} samples, mean target {T.mean():.3f}")
         model = train(X, T, epochs=args.epochs, batch=args.batch, lr=args.lr, over=args.over, log=log)
-        model.meta["train_graphs"] = [[n, s] for n, _, ss in TRAIN_GRAPHS for s in ss]
+        model.meta["train_graphs"] = [[n, s, walk_seed(s)] for n, _, walk_seed, ss in TRAIN_GRAPHS for s in ss]
+        model.meta["per_round"] = args.per_round
         model.save(args.out)
         report["train"] = model.meta
         if args.eval:
