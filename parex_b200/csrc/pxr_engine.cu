@@ -377,6 +377,8 @@ struct pxr_handle {
     // learned sweep schedule
     pxr_schedule sched{};
     uint8_t* sflag = nullptr;
+    uint32_t* smax = nullptr;
+    uint32_t* smin = nullptr;
     uint8_t* nflag = nullptr;
     uint32_t* rootc = nullptr;
     float* mlp = nullptr;             // kMlpImage floats
@@ -503,6 +505,8 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.sched = h->sched.mode;
     d.trace = (h->sched.trace && h->records) ? 1u : 0u;
     d.sflag = h->sflag;
+    d.smax = h->smax;
+    d.smin = h->smin;
     d.nflag = h->nflag;
     d.rootc = h->rootc;
     d.lb_sched = h->lb[kSiteSched];
@@ -685,7 +689,8 @@ cudaError_t op_sweep(pxr_handle* h) {
     phase(h, kPhBook, 1, [&] { launch_pdl(k_round_prep<OffT>, 1, 32, 0, s, d, 1, c_gsort, c_chunk); });
     const uint32_t tiles = std::max((h->n + kScanTile - 1) / kScanTile, 1u);
     if (h->sched.mode)
-        phase(h, kPhSched, 2, [&] {
+        phase(h, kPhSched, 3, [&] {
+            launch_pdl(k_cluster_spread<OffT>, std::min(tiles, kMaxGrid), kBlock, 0, s, d, h->ids[h->acur]);
             launch_pdl(k_due_scan<OffT>, tiles, kBlock, 0, s, d, t);
             launch_pdl(k_walk_only_check<OffT>, 1, 1, 0, s, d);
         });
@@ -1003,6 +1008,7 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
         A(&h->tab[i].root, N); A(&h->tab[i].best, N); A(&h->tab[i].skip, N); A(&h->tab[i].hist, N);
     }
     A(&h->sflag, N); A(&h->nflag, N); A(&h->rootc, N); A(&h->mlp, (size_t)kMlpImage);
+    A(&h->smax, N); A(&h->smin, N);
     if (h->sched.trace) { A(&h->records, N); }
     A(&h->cut_off, N); A(&h->split, N); A(&h->allcuts, N); A(&h->rep[0], N); A(&h->rep[1], N);
     A(&h->walk_stats, 3 * kStatSlots);
@@ -1034,6 +1040,8 @@ pxr_status allocate(pxr_handle* h, uint32_t n, uint64_t m) {
     cudaStream_t s = h->stream;
     for (int i = 0; i <= kSiteRoots; ++i) PXR_CUDA(h, cudaMemsetAsync(h->lb[i].flags, 0, scan_tiles * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->rootmap, 0, (N / 32 + 1) * 4, s));
+    PXR_CUDA(h, cudaMemsetAsync(h->smax, 0, N * 4, s));      // per-label spread: identity
+    PXR_CUDA(h, cudaMemsetAsync(h->smin, 0xFF, N * 4, s));
     PXR_CUDA(h, cudaMemsetAsync(h->walk_stats, 0, 3 * kStatSlots * sizeof(unsigned long long), s));
     PXR_CUDA(h, cudaMemsetAsync(h->lb_epoch, 0, kSites * 4, s));
     h->records_n = h->records ? (uint32_t)N : 0u;

@@ -171,6 +171,7 @@ __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle 
     c->n_active_next = 0;
     if (stage == 1) {
         c->n_due_items = 0;
+        c->any_split = 0;
         if (d.sched) c->n_sweep = 0;   // set by k_due_scan
     }
     if (!d.sched) c->n_sweep = c->n_active;
@@ -520,6 +521,9 @@ __global__ void __launch_bounds__(kBlock) k_cluster_cut(Dev<OffT> d, ClusterTabl
         d.cut_off[c] = cut ? off : kNoCut;
         const bool split = acted && (cut || full);
         d.split[c] = split ? 1 : 0;
+        const uint32_t am = __activemask();
+        const uint32_t splits = __ballot_sync(am, split);
+        if (split && (splits & lanemask_lt()) == 0u) d.ctr->any_split = 1u;   // one store per warp
         const uint32_t cuts_in_warp = __ballot_sync(__activemask(), cut);
         if (cut && (cuts_in_warp & lanemask_lt()) == 0u) atomicAdd(&d.ctr->n_cut, (uint32_t)__popc(cuts_in_warp));
         if (!acted && swept && sp < d.sc_threshold) atomicAdd(&d.ctr->stat_false_stops, 1ull);
@@ -602,6 +606,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_link_first(Dev<OffT> d, const uint32_t* ids) {
     pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
+    if (!d.ctr->any_split) return;   // no cluster split: no components to find
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
@@ -629,6 +634,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_compress(Dev<OffT> d, const uint32_t* ids) {
     pdl_wait();
     if (d.ctr->walk_only) return;
+    if (!d.ctr->any_split) return;   // no cluster split: no components to find
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
@@ -666,6 +672,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_union_sample(Dev<OffT> d, const uint32_t* ids) {
     pdl_wait();
     if (d.ctr->walk_only) return;
+    if (!d.ctr->any_split) return;   // no cluster split: no components to find
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) {
@@ -687,7 +694,7 @@ template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_union_reps(Dev<OffT> d, ClusterTables t, const uint32_t* vals0,
                                                        const uint32_t* vals1) {
     pdl_wait();
-    if (d.ctr->walk_only) return;
+    if (d.ctr->walk_only || !d.ctr->any_split) return;
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t* vals = d.ctr->main_sel ? vals1 : vals0;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < k; c += gridDim.x * blockDim.x) {
@@ -722,7 +729,7 @@ __device__ __forceinline__ bool union_skip_row(const Dev<OffT>& d, uint32_t k, u
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_union(Dev<OffT> d, const uint32_t* ids) {
     pdl_wait();
-    if (d.ctr->walk_only) return;
+    if (d.ctr->walk_only || !d.ctr->any_split) return;
     const uint32_t count = d.ctr->n_active;
     const uint32_t k = d.ctr->n_clusters;
     const uint32_t gl = threadIdx.x & (W - 1);
@@ -936,7 +943,8 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
                 nt.vol[nl] = kind == kOriginChild ? 0u : t.vol[c];
                 if (kind == kOriginCarried) {
                     const uint16_t sk = t.skip[c];
-                    nt.skip[nl] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+                    // due next round once its spread is below the threshold (k_due_scan)
+                    nt.skip[nl] = (sk > 0 && !(d.sflag[c] & 4u)) ? (uint16_t)(sk - 1u) : (uint16_t)0u;
                     nt.hist[nl] = t.hist[c];
                 }
             } else {
@@ -1308,7 +1316,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
 template <typename OffT, int G>
 __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
     pdl_wait();
-    if (d.ctr->walk_only) return;   // nothing due: the round only walks
+    if (d.ctr->walk_only || !d.ctr->any_split) return;   // nothing due, or nothing split
     const uint32_t k = d.ctr->n_clusters;
     uint32_t cnt;
     const uint32_t* list = row_list(d, G, &cnt);

@@ -110,7 +110,10 @@ struct Dev {
     // learned sweep schedule (all zero / null in the plain form)
     uint32_t sched;           // PXR_SCHEDULE_*
     uint32_t trace;           // write per-cluster records each round
-    uint8_t* sflag;           // per label this round: bit 0 acted on (due), bit 1 in the sweep
+    uint8_t* sflag;           // per label this round: bit 0 acted on (due), bit 1 in the sweep,
+                              // bit 2 carried with its potential spread already below rw_threshold
+    uint32_t* smax;           // per label: max / min ordered potential bits after this round's walk
+    uint32_t* smin;           // (learned schedule; identity between rounds)
     uint8_t* nflag;           // per label of the next round: kRows* (rows to rescan or not)
     uint32_t* rootc;          // per root vertex: kind << 30 | old label
     LookbackState lb_sched, lb_emit, lb_carry;

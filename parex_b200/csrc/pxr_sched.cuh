@@ -20,6 +20,69 @@
 
 namespace pxr {
 
+// Potential spread per cluster after the walk, over the active list in vertex
+// order (runs of one label give few atomics).  A carried cluster whose spread
+// is already below rw_threshold is swept in the next round instead of
+// walking until its skip counter runs out: the keep test would certify it,
+// and every further walk step over it is wasted.
+struct SpreadAgg {
+    using T = uint2;              // x: max ordered bits, y: min ordered bits
+    uint32_t* smax;
+    uint32_t* smin;
+    __device__ static T identity() { return make_uint2(0u, 0xFFFFFFFFu); }
+    __device__ static T combine(T a, T b) { return make_uint2(a.x > b.x ? a.x : b.x, a.y < b.y ? a.y : b.y); }
+    __device__ static T warp_reduce(T v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            T u;
+            u.x = __shfl_xor_sync(0xFFFFFFFFu, v.x, o);
+            u.y = __shfl_xor_sync(0xFFFFFFFFu, v.y, o);
+            v = combine(v, u);
+        }
+        return v;
+    }
+    __device__ void emit(uint32_t key, T v) const {
+        atomicMax(&smax[key], v.x);
+        atomicMin(&smin[key], v.y);
+    }
+};
+
+template <typename OffT>
+__global__ void __launch_bounds__(kBlock) k_cluster_spread(Dev<OffT> d, const uint32_t* ids) {
+    pdl_wait();
+    const uint32_t count = d.ctr->n_active;
+    const uint32_t k = d.ctr->n_clusters;
+    SpreadAgg agg{d.smax, d.smin};
+    const uint32_t stride = gridDim.x * kScanTile;
+    for (uint32_t base = blockIdx.x * kScanTile; base < count; base += stride) {
+        const uint32_t first = base + threadIdx.x * kScanItems;
+        bool has = false, single = true;
+        uint32_t k_first = 0, k_last = 0;
+        uint2 a_first = SpreadAgg::identity(), a_last = SpreadAgg::identity();
+        for (int q = 0; q < kScanItems; ++q) {
+            const uint32_t j = first + q;
+            if (j >= count) break;
+            const uint32_t v = ids[j];
+            const uint32_t c = (uint32_t)d.lab[v];
+            if (c >= k) continue;
+            const uint32_t ob = ordered_bits(d.x[v]);
+            const uint2 cur = make_uint2(ob, ob);
+            if (!has) {
+                has = true; k_first = c; a_first = cur; k_last = c; a_last = cur;
+            } else if (c == k_last) {
+                a_last = SpreadAgg::combine(a_last, cur);
+                if (single) a_first = a_last;
+            } else {
+                if (!single) agg.emit(k_last, a_last);
+                single = false;
+                k_last = c;
+                a_last = cur;
+            }
+        }
+        emit_fragments<SpreadAgg>(has, single, k_first, a_first, k_last, a_last, agg);
+    }
+}
+
 // per cluster: due / in-sweep flags and the start tables of the sweep set
 template <typename OffT>
 __global__ void __launch_bounds__(kBlock) k_due_scan(Dev<OffT> d, ClusterTables t) {
@@ -42,7 +105,11 @@ __global__ void __launch_bounds__(kBlock) k_due_scan(Dev<OffT> d, ClusterTables 
         if (c < count) {
             const bool due = t.skip[c] == 0;
             const bool swept = due || d.sched == 2u;
-            d.sflag[c] = (uint8_t)((due ? 1u : 0u) | (swept ? 2u : 0u));
+            const float spread = __fsub_rn(from_ordered_bits(d.smax[c]), from_ordered_bits(d.smin[c]));
+            const bool settled = !due && d.smin[c] != 0xFFFFFFFFu && spread < d.rw_threshold;
+            d.smax[c] = 0u;              // identity again for the next round
+            d.smin[c] = 0xFFFFFFFFu;
+            d.sflag[c] = (uint8_t)((due ? 1u : 0u) | (swept ? 2u : 0u) | (settled ? 4u : 0u));
             if (swept) v = ((uint64_t)t.vol[c] << 32) | t.size[c];
             if (due) due_items += t.size[c]; else ++skipped;
         }
@@ -159,7 +226,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_all(Dev<OffT> d, ClusterTables
         nt.root[c] = t.root[c];
         nt.best[c] = ~0ull;
         const uint16_t sk = t.skip[c];
-        nt.skip[c] = sk > 0 ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+        nt.skip[c] = (sk > 0 && !(d.sflag[c] & 4u)) ? (uint16_t)(sk - 1u) : (uint16_t)0u;
         nt.hist[c] = t.hist[c];
         if (d.trace) {
             pxr_cluster_record& o = static_cast<pxr_cluster_record*>(d.records)[c];
