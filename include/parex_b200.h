@@ -404,6 +404,26 @@ pxr_status pxr_test_bounded_waits(pxr_handle* h, uint32_t spin_limit, uint32_t* 
 size_t pxr_build_csr_scratch_bytes(uint64_t n_edges);
 pxr_status pxr_build_csr(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
                          uint32_t* offsets, uint32_t* cols, uint64_t* m_out, void* stream);
+/* The CSR of the reference's own input path, on the device:
+ * DynamicGraph::finalize (lib/core/graph.h:147-184) keeps the edge list as it
+ * stands - duplicate edges and self-loops included (a self-loop gives two
+ * slots in its row) - and stores both directions, rows sorted by neighbour.
+ * Same arguments and scratch as pxr_build_csr; the graph has m = n_edges.
+ * Needs 2 * n_edges < 2^32 (the reference's 32-bit EdgeIx). */
+pxr_status pxr_build_csr_finalize(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
+                                  uint32_t* offsets, uint32_t* cols, void* stream);
+/* The body of a Matrix Market file (device memory: the bytes after the size
+ * line) parsed as readDynGraph (lib/utils/graph_io.h:49-84) reads it: a stream
+ * of decimal integers, two per edge, 1-based, line breaks not significant;
+ * the first 2 * n_edges numbers give u[i], v[i] (0-based).  The caller
+ * parses the header (comment lines, then "rows n n_edges") on the host.
+ * scratch: pxr_parse_mtx_scratch_bytes(text_bytes) bytes of device memory.
+ * *tokens_out: the numbers found.  PXR_INVALID_ARG when fewer than
+ * 2 * n_edges numbers are found or an id lies outside 1..n (the reference
+ * would read past its edge array or wrap).  Synchronises the stream. */
+size_t pxr_parse_mtx_scratch_bytes(uint64_t text_bytes);
+pxr_status pxr_parse_mtx_body(const char* text, uint64_t text_bytes, uint32_t n, uint64_t n_edges, uint32_t* u,
+                              uint32_t* v, void* scratch, uint64_t* tokens_out, void* stream);
 /* One block pair of a planted-partition instance: candidate pairs
  * (base_u + i, base_v + j), i < su, j < sv (intra: i < j < su, base_u == base_v),
  * each an edge with probability p.  key names the task's random stream: a

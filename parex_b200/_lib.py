@@ -33,7 +33,8 @@ SYMBOLS = [
     "pxr_set_schedule", "pxr_read_cluster_records", "pxr_mlp_forward", "pxr_mlp_scratch_floats", "pxr_mlp_gradient",
     "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
     "pxr_rmat_edges", "pxr_sbm_edges", "pxr_initialize_batched_device", "pxr_test_bounded_waits",
-    "pxr_get_sort_plan", "pxr_set_sort_plan",
+    "pxr_get_sort_plan", "pxr_set_sort_plan", "pxr_build_csr_finalize", "pxr_parse_mtx_scratch_bytes",
+    "pxr_parse_mtx_body",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -170,6 +171,10 @@ def load() -> C.CDLL:
     L.pxr_count_cut_edges.argtypes = [p, C.POINTER(u64)]
     L.pxr_test_bounded_waits.argtypes = [p, u32, C.POINTER(u32)]
     L.pxr_get_sort_plan.argtypes = [p, C.POINTER(SortPlan)]
+    L.pxr_build_csr_finalize.argtypes = [u32, u64, p, p, p, p, p, p]
+    L.pxr_parse_mtx_scratch_bytes.argtypes = [u64]
+    L.pxr_parse_mtx_scratch_bytes.restype = C.c_size_t
+    L.pxr_parse_mtx_body.argtypes = [p, u64, u32, u64, p, p, p, C.POINTER(u64), p]
     L.pxr_set_sort_plan.argtypes = [p, C.POINTER(SortPlan)]
     L.pxr_download_certificates.argtypes = [p, p]
     L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]

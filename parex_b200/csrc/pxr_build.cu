@@ -169,6 +169,84 @@ __global__ void k_sbm_segments(const pxr_sbm_task* tasks, uint32_t n_tasks, cons
 
 __global__ void k_set_u32(uint32_t* p, uint32_t value) { *p = value; }
 
+// DynamicGraph::finalize (lib/core/graph.h:147-184): both directions of every
+// edge as it stands - self-loops and duplicate edges kept - sorted by
+// (from, to) by the radix sort that follows.
+__global__ void k_both_directions(const uint32_t* u, const uint32_t* v, uint64_t n_edges, uint32_t n, uint64_t* keys,
+                                  uint32_t* bad) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_edges;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = u[i], b = v[i];
+        if (a >= n || b >= n) { atomicOr(bad, 1u); keys[2 * i] = keys[2 * i + 1] = 0; continue; }
+        keys[2 * i] = ((uint64_t)a << 32) | b;
+        keys[2 * i + 1] = ((uint64_t)b << 32) | a;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Matrix Market body on the device.  readDynGraph (lib/utils/graph_io.h:49-84)
+// reads the body as a stream of integers, "fx tx" per edge, 1-based, with no
+// regard to lines; so does this tokenizer: a token is a maximal run of
+// decimal digits, tokens 2i and 2i+1 are edge i.  Each thread owns
+// kMtxBytes bytes and parses the tokens that start there (reading past its
+// bytes to a token's end); a tile's tokens are numbered by a decoupled
+// look-back over tile counts (tile ids taken in launch order).
+
+constexpr uint32_t kMtxBytes = 16;
+constexpr uint32_t kMtxTile = kBuildBlock * kMtxBytes;
+
+__device__ __forceinline__ bool is_digit(unsigned char c) { return c >= '0' && c <= '9'; }
+
+__global__ void __launch_bounds__(kBuildBlock) k_mtx_tokens(const unsigned char* text, uint64_t len, uint64_t n_edges,
+                                                            uint32_t n, uint32_t* u, uint32_t* v, uint32_t* tile_ctr,
+                                                            LookbackState lb, unsigned long long* tokens_out,
+                                                            uint32_t* bad, uint32_t* err) {
+    __shared__ uint64_t warp_tot[kBuildBlock / 32];
+    __shared__ uint64_t s_excl;
+    __shared__ uint32_t s_tile;
+    const uint64_t ntiles = (len + kMtxTile - 1) / kMtxTile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile >= ntiles) return;
+    const uint64_t b0 = (uint64_t)tile * kMtxTile + (uint64_t)threadIdx.x * kMtxBytes;
+    uint32_t starts = 0;
+    for (uint32_t q = 0; q < kMtxBytes; ++q) {
+        const uint64_t i = b0 + q;
+        if (i >= len) break;
+        if (is_digit(text[i]) && (i == 0 || !is_digit(text[i - 1]))) starts |= 1u << q;
+    }
+    const uint32_t cnt = __popc(starts);
+    uint64_t total;
+    const uint64_t incl = block_inclusive<Add64>((uint64_t)cnt, warp_tot, &total);
+    if (threadIdx.x < 32) {
+        const uint64_t ex = lookback_tile<Add64>(lb, tile, 1u, total, err);
+        if (threadIdx.x == 0) {
+            s_excl = ex;
+            if (tile == ntiles - 1) *tokens_out = ex + total;
+        }
+    }
+    __syncthreads();
+    uint64_t k = s_excl + incl - cnt;
+    while (starts) {
+        const uint32_t q = (uint32_t)__ffs(starts) - 1u;
+        starts &= starts - 1u;
+        uint64_t val = 0;
+        bool big = false;
+        for (uint64_t i = b0 + q; i < len && is_digit(text[i]); ++i) {
+            val = val * 10u + (text[i] - '0');
+            if (val > 0xFFFFFFFFull) { big = true; val = 0xFFFFFFFFull; }
+        }
+        if (k < 2 * n_edges) {
+            // 1-based ids; 0 or ids above n have no vertex
+            if (big || val == 0 || val > n) atomicOr(bad, 1u);
+            const uint32_t id = (val >= 1 && val <= n) ? (uint32_t)(val - 1) : 0u;
+            if (k & 1u) v[k >> 1] = id; else u[k >> 1] = id;
+        }
+        ++k;
+    }
+}
+
 struct BuildLayout {
     size_t keys0, keys1, hist, bases, pass_info, tile_ctr, epoch, status, words, total;
     uint32_t tiles;
@@ -229,6 +307,94 @@ pxr_status pxr_sbm_edges(const pxr_sbm_task* tasks, uint32_t n_tasks, const uint
 }
 
 size_t pxr_build_csr_scratch_bytes(uint64_t n_edges) { return build_layout(n_edges).total; }
+
+size_t pxr_parse_mtx_scratch_bytes(uint64_t text_bytes) {
+    const uint64_t slots = (text_bytes + kMtxTile - 1) / kMtxTile + 1;   // look-back state per tile
+    return 256 + align256(slots * 4) + 2 * align256(slots * 8);
+}
+
+pxr_status pxr_parse_mtx_body(const char* text, uint64_t text_bytes, uint32_t n, uint64_t n_edges, uint32_t* u,
+                              uint32_t* v, void* scratch, uint64_t* tokens_out, void* stream) {
+    if (!tokens_out || (text_bytes && (!text || !scratch)) || (n_edges && (!u || !v))) return PXR_INVALID_ARG;
+    *tokens_out = 0;
+    if (!text_bytes) return n_edges ? PXR_INVALID_ARG : PXR_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint64_t tiles = (text_bytes + kMtxTile - 1) / kMtxTile;
+    if (tiles >= (1ull << 32)) return PXR_INVALID_ARG;
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    // words: tile counter, bad, err, pad | tokens (u64) | flags | agg | inc
+    uint32_t* words = reinterpret_cast<uint32_t*>(base);
+    unsigned long long* tokens = reinterpret_cast<unsigned long long*>(base + 16);
+    LookbackState lb{};
+    lb.flags = reinterpret_cast<uint32_t*>(base + 256);
+    lb.agg = reinterpret_cast<uint64_t*>(base + 256 + align256((tiles + 1) * 4));
+    lb.inc = reinterpret_cast<uint64_t*>(base + 256 + align256((tiles + 1) * 4) + align256((tiles + 1) * 8));
+    if (cudaMemsetAsync(base, 0, 256 + align256((tiles + 1) * 4), s) != cudaSuccess) return PXR_CUDA_ERROR;
+    k_mtx_tokens<<<(uint32_t)tiles, kBuildBlock, 0, s>>>(reinterpret_cast<const unsigned char*>(text), text_bytes,
+                                                         n_edges, n, u, v, &words[0], lb, tokens, &words[1],
+                                                         &words[2]);
+    if (cudaGetLastError() != cudaSuccess) return PXR_CUDA_ERROR;
+    uint32_t w[3] = {0, 0, 0};
+    unsigned long long t = 0;
+    if (cudaMemcpyAsync(w, words, 12, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaMemcpyAsync(&t, tokens, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    *tokens_out = t;
+    if (w[2]) return PXR_DEVICE_FAULT;        // a look-back wait ran out
+    if (t < 2 * n_edges || w[1]) return PXR_INVALID_ARG;   // too few numbers, or an id outside 1..n
+    return PXR_OK;
+}
+
+pxr_status pxr_build_csr_finalize(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
+                                  uint32_t* offsets, uint32_t* cols, void* stream) {
+    if (!offsets || (n_edges && (!u || !v || !cols || !scratch))) return PXR_INVALID_ARG;
+    if (n >= 0x7FFFFFFFu || 2 * n_edges >= (1ull << 32)) return PXR_INVALID_ARG;   // 32-bit offsets (EdgeIx)
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    static bool prepared[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (dev >= 0 && dev < 64 && !prepared[dev]) {
+        if (radix_sort_prepare<uint64_t>() != cudaSuccess) return PXR_CUDA_ERROR;
+        prepared[dev] = true;
+    }
+    const BuildLayout L = build_layout(n_edges);
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    uint64_t* k0 = reinterpret_cast<uint64_t*>(base + L.keys0);
+    uint64_t* k1 = reinterpret_cast<uint64_t*>(base + L.keys1);
+    uint32_t* words = reinterpret_cast<uint32_t*>(base + L.words);
+    uint32_t *count1 = words + 1, *end_bit = words + 2, *err = words + 3, *bad = words + 4;
+    if (cudaMemsetAsync(base + L.hist, 0, L.total - L.hist, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    uint32_t bits = 0;
+    while (bits < 32 && (1ull << bits) < n) ++bits;
+    k_set_u32<<<1, 1, 0, s>>>(end_bit, 32u + bits);
+    k_set_u32<<<1, 1, 0, s>>>(count1, (uint32_t)(2 * n_edges));
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((std::max<uint64_t>(n_edges, (uint64_t)n + 1) + kBuildBlock - 1) /
+                                                           kBuildBlock, 148u * 32u);
+    if (n_edges) k_both_directions<<<grid, kBuildBlock, 0, s>>>(u, v, n_edges, n, k0, bad);
+    SortState st{};
+    st.hist = reinterpret_cast<uint32_t*>(base + L.hist);
+    st.bases = reinterpret_cast<uint32_t*>(base + L.bases);
+    st.pass_info = reinterpret_cast<uint32_t*>(base + L.pass_info);
+    st.tile_ctr = reinterpret_cast<uint32_t*>(base + L.tile_ctr);
+    st.epoch = reinterpret_cast<uint32_t*>(base + L.epoch);
+    st.status = reinterpret_cast<uint64_t*>(base + L.status);
+    st.max_tiles = L.tiles;
+    st.items_moved = nullptr;
+    SortBuffers<uint64_t> b{};
+    b.keys[0] = k0;
+    b.keys[1] = k1;
+    b.count = count1;
+    b.end_bit = end_bit;
+    b.capacity = (uint32_t)(2 * n_edges);
+    if (radix_sort<uint64_t>(b, st, err, s, 64) != cudaSuccess) return PXR_CUDA_ERROR;
+    k_csr_rows<<<grid, kBuildBlock, 0, s>>>(k0, k1, st.pass_info + kMaxPasses, count1, n, offsets, cols);
+    uint32_t w[5] = {0, 0, 0, 0, 0};
+    if (cudaMemcpyAsync(w, words, 20, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (w[4]) return PXR_INVALID_ARG;   // a vertex id >= n
+    if (w[3]) return PXR_DEVICE_FAULT;  // a sort wait ran out
+    return PXR_OK;
+}
 
 pxr_status pxr_build_csr(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
                          uint32_t* offsets, uint32_t* cols, uint64_t* m_out, void* stream) {

@@ -694,16 +694,25 @@ cudaError_t op_sweep(pxr_handle* h) {
             launch_pdl(k_due_scan<OffT>, tiles, kBlock, 0, s, d, t);
             launch_pdl(k_walk_only_check<OffT>, 1, 1, 0, s, d);
         });
-    phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
-        launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur]);
-        PXR_LONG(h, k_nodediff_long, d);
-    });
-    phase(h, kPhEmit, 1, [&] {
-        if (h->sched.mode)
+    // learned schedule: the sweep set is compacted first and the edge
+    // differences are taken over it alone (carried clusters need none)
+    if (h->sched.mode) {
+        phase(h, kPhEmit, 1, [&] {
             launch_pdl(k_emit_sched<OffT>, tiles, kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
-        else
+        });
+        phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
+            launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->vals[0], 1);
+            PXR_LONG(h, k_nodediff_long, d);
+        });
+    } else {
+        phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
+            launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur], 0);
+            PXR_LONG(h, k_nodediff_long, d);
+        });
+        phase(h, kPhEmit, 1, [&] {
             launch_pdl(k_emit<OffT>, grid_for(h->n), kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
-    });
+        });
+    }
     SortBuffers<uint64_t> b{};
     b.keys[0] = h->keys[0]; b.keys[1] = h->keys[1];
     b.vals[0] = h->vals[0]; b.vals[1] = h->vals[1];

@@ -346,11 +346,14 @@ __global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* id
 // edge differences (nodeDiffKernel_Sparse_WarpParallel, cuda/devSweepCut.h:20-112):
 // +1 per valid neighbour after v in (potential, id) order, -1 per neighbour before.
 
+// ids: the active list in vertex order (count n_active), or with sweep_list
+// the sweep set as the learned schedule's emit compacted it (count n_sweep,
+// every entry swept).
 template <typename OffT, int W>
-__global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t* ids) {
+__global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t* ids, int sweep_list = 0) {
     pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
-    const uint32_t count = d.ctr->n_active;
+    const uint32_t count = sweep_list ? d.ctr->n_sweep : d.ctr->n_active;
     const uint32_t gl = threadIdx.x & (W - 1);
     const uint32_t groups = (gridDim.x * blockDim.x) / W;
     const uint32_t warp0 = ((blockIdx.x * blockDim.x + threadIdx.x) & ~31u) / W;
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t
         const uint32_t j = j0 + (threadIdx.x & 31u) / W;
         const bool valid = j < count;
         uint32_t v = valid ? ids[j] : 0u;
-        const bool in = valid && (!d.sched || ((uint32_t)d.lab[v] < d.n && (d.sflag[d.lab[v]] & 2u)));
+        const bool in = valid && (sweep_list || !d.sched || ((uint32_t)d.lab[v] < d.n && (d.sflag[d.lab[v]] & 2u)));
         if (!in) v = 0u;
         const uint32_t mine = in ? ordered_bits(d.x[v]) : 0u;
         OffT beg = in ? d.off[v] : 0, end = in ? d.off[v + 1] : 0;

@@ -40,6 +40,70 @@ def build_csr(n: int, u, v, device: int = 0):
     return offsets, cols[: 2 * m.value], m.value
 
 
+def build_csr_finalize(n: int, u, v, device: int = 0):
+    """(offsets, cols, m) on the device with the reference's finalize
+    semantics (pxr_build_csr_finalize): duplicates and self-loops kept, both
+    directions, rows sorted; m = number of input edges."""
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda", device)
+    n_edges = int(u.shape[0])
+    scratch = torch.empty(max(int(L.pxr_build_csr_scratch_bytes(n_edges)), 1), dtype=torch.uint8, device=dev)
+    offsets = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    cols = torch.empty(max(2 * n_edges, 1), dtype=torch.int32, device=dev)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    st = L.pxr_build_csr_finalize(n, n_edges, _p(u) if n_edges else None, _p(v) if n_edges else None, _p(scratch),
+                                  _p(offsets), _p(cols), stream)
+    if st != 0:
+        raise _lib.PxrError(st, "pxr_build_csr_finalize")
+    return offsets, cols[: 2 * n_edges], n_edges
+
+
+def mtx_header(data: bytes):
+    """(rows, n, n_edges, body offset) of a Matrix Market file's bytes: comment
+    lines start with '%'; the first other line holds three integers, of which
+    readDynGraph (lib/utils/graph_io.h:49-84) takes the second as the vertex
+    count and the third as the edge count."""
+    pos = 0
+    while True:
+        end = data.find(b"\n", pos)
+        line = data[pos:] if end < 0 else data[pos:end]
+        if not line.lstrip().startswith(b"%"):
+            fields = line.split()
+            if len(fields) < 3:
+                raise ValueError("Matrix Market size line needs three integers")
+            return int(fields[0]), int(fields[1]), int(fields[2]), (len(data) if end < 0 else end + 1)
+        if end < 0:
+            raise ValueError("no size line")
+        pos = end + 1
+
+
+def read_mtx(path, device: int = 0):
+    """A Matrix Market graph read as the reference's readDynGraph +
+    DynamicGraph::finalize read it, with the body tokenised and the CSR built
+    on the device: (offsets, cols, n, m) as torch tensors / ints."""
+    import torch
+    L = _lib.load()
+    dev = torch.device("cuda", device)
+    with open(path, "rb") as f:
+        data = f.read()
+    _, n, n_edges, body = mtx_header(data)
+    text = torch.frombuffer(bytearray(data[body:]) if body < len(data) else bytearray(1), dtype=torch.uint8)
+    text_d = text.to(dev)
+    nbytes = len(data) - body
+    u = torch.empty(max(n_edges, 1), dtype=torch.int32, device=dev)
+    v = torch.empty(max(n_edges, 1), dtype=torch.int32, device=dev)
+    scratch = torch.empty(max(int(L.pxr_parse_mtx_scratch_bytes(nbytes)), 1), dtype=torch.uint8, device=dev)
+    tokens = C.c_uint64(0)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    st = L.pxr_parse_mtx_body(_p(text_d), nbytes, n, n_edges, _p(u), _p(v), _p(scratch), C.byref(tokens), stream)
+    if st != 0:
+        raise _lib.PxrError(st, f"pxr_parse_mtx_body ({tokens.value} numbers for {n_edges} edges)")
+    del text_d, scratch
+    offsets, cols, m = build_csr_finalize(n, u[:n_edges], v[:n_edges], device)
+    return offsets, cols, n, m
+
+
 def rmat_edges(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1,
                device: int = 0):
     import torch
