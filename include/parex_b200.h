@@ -424,6 +424,22 @@ pxr_status pxr_build_csr_finalize(uint32_t n, uint64_t n_edges, const uint32_t* 
 size_t pxr_parse_mtx_scratch_bytes(uint64_t text_bytes);
 pxr_status pxr_parse_mtx_body(const char* text, uint64_t text_bytes, uint32_t n, uint64_t n_edges, uint32_t* u,
                               uint32_t* v, void* scratch, uint64_t* tokens_out, void* stream);
+/* One level of the expander hierarchy on the device
+ * (ExpanderHierarchy::contract, lib/algorithms/expander_hierarchy.h:34-88):
+ * the graph whose vertices are the k clusters of `ids` (n int32 in [0, k),
+ * e.g. pxr_final_partition's ids) and whose edges are the cut edges of the
+ * level graph (offsets/cols: n + 1 and offsets[n] 32-bit entries), one per cut
+ * edge, multi-edges kept, rows sorted (the reference leaves them in its
+ * clusters' vertex order).  cut_sizes[c]: cut slots leaving cluster c;
+ * volumes[c]: sum over its vertices of level_volumes (k 64-bit entries; at the
+ * first level pass NULL to take the vertices' degrees).  out_offsets: k + 1
+ * entries; out_cols: room for offsets[n] entries; *out_m: edges of the
+ * contracted graph.  All arrays in device memory; scratch:
+ * pxr_contract_scratch_bytes(offsets[n]) bytes.  Synchronises the stream. */
+size_t pxr_contract_scratch_bytes(uint64_t slots);
+pxr_status pxr_contract(uint32_t n, const uint32_t* offsets, const uint32_t* cols, const int32_t* ids, uint32_t k,
+                        const uint64_t* level_volumes, void* scratch, uint32_t* out_offsets, uint32_t* out_cols,
+                        uint64_t* out_m, uint64_t* cut_sizes, uint64_t* volumes, void* stream);
 /* One block pair of a planted-partition instance: candidate pairs
  * (base_u + i, base_v + j), i < su, j < sv (intra: i < j < su, base_u == base_v),
  * each an edge with probability p.  key names the task's random stream: a

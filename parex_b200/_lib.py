@@ -34,7 +34,7 @@ SYMBOLS = [
     "pxr_mlp_adam_step", "pxr_get_row_plan", "pxr_set_row_plan", "pxr_build_csr_scratch_bytes", "pxr_build_csr",
     "pxr_rmat_edges", "pxr_sbm_edges", "pxr_initialize_batched_device", "pxr_test_bounded_waits",
     "pxr_get_sort_plan", "pxr_set_sort_plan", "pxr_build_csr_finalize", "pxr_parse_mtx_scratch_bytes",
-    "pxr_parse_mtx_body",
+    "pxr_parse_mtx_body", "pxr_contract_scratch_bytes", "pxr_contract",
 ]
 STATIC_SCRATCH_MAX_LABELS = 65536
 
@@ -175,6 +175,9 @@ def load() -> C.CDLL:
     L.pxr_parse_mtx_scratch_bytes.argtypes = [u64]
     L.pxr_parse_mtx_scratch_bytes.restype = C.c_size_t
     L.pxr_parse_mtx_body.argtypes = [p, u64, u32, u64, p, p, p, C.POINTER(u64), p]
+    L.pxr_contract_scratch_bytes.argtypes = [u64]
+    L.pxr_contract_scratch_bytes.restype = C.c_size_t
+    L.pxr_contract.argtypes = [u32, p, p, p, u32, p, p, p, p, C.POINTER(u64), p, p, p]
     L.pxr_set_sort_plan.argtypes = [p, C.POINTER(SortPlan)]
     L.pxr_download_certificates.argtypes = [p, p]
     L.pxr_num_active_clusters.argtypes = [p, C.POINTER(u32)]

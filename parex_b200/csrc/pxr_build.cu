@@ -272,6 +272,39 @@ BuildLayout build_layout(uint64_t n_edges) {
     return L;
 }
 
+// Expander hierarchy contraction (ExpanderHierarchy::contract,
+// lib/algorithms/expander_hierarchy.h:34-88): one warp per vertex; every slot
+// whose ends lie in different clusters becomes a (cluster, neighbour's
+// cluster) key of the contracted graph and counts toward its cluster's cut;
+// the cluster's volume adds the vertex's volume (its degree at the first
+// level, its subtree volume above).
+__global__ void k_contract_slots(uint32_t n, const uint32_t* off, const uint32_t* cols, const int32_t* ids,
+                                 uint32_t k, const unsigned long long* level_vol, uint64_t* keys, uint32_t* count,
+                                 unsigned long long* cut_sizes, unsigned long long* volumes, uint32_t* bad) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        const int32_t c = ids[v];
+        if (c < 0 || (uint32_t)c >= k) { if (lane == 0) atomicOr(bad, 1u); continue; }
+        const uint32_t beg = off[v], end = off[v + 1];
+        uint32_t cut = 0;
+        for (uint32_t s = beg + lane; s < end; s += 32) {
+            const uint32_t u = cols[s];
+            if (u >= n) { atomicOr(bad, 1u); continue; }
+            const int32_t cu = ids[u];
+            if (cu == c) continue;
+            ++cut;
+            keys[atomicAdd(count, 1u)] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)cu;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cut += __shfl_xor_sync(0xFFFFFFFFu, cut, o);
+        if (lane == 0) {
+            if (cut) atomicAdd(&cut_sizes[c], (unsigned long long)cut);
+            atomicAdd(&volumes[c], level_vol ? level_vol[v] : (unsigned long long)(end - beg));
+        }
+    }
+}
+
 }  // namespace
 }  // namespace pxr
 
@@ -344,6 +377,70 @@ pxr_status pxr_parse_mtx_body(const char* text, uint64_t text_bytes, uint32_t n,
     if (t < 2 * n_edges || w[1]) return PXR_INVALID_ARG;   // too few numbers, or an id outside 1..n
     return PXR_OK;
 }
+
+pxr_status pxr_contract(uint32_t n, const uint32_t* offsets, const uint32_t* cols, const int32_t* ids, uint32_t k,
+                        const uint64_t* level_volumes, void* scratch, uint32_t* out_offsets, uint32_t* out_cols,
+                        uint64_t* out_m, uint64_t* cut_sizes, uint64_t* volumes, void* stream) {
+    if (!offsets || !ids || !out_offsets || !out_m || !cut_sizes || !volumes || !scratch || k == 0 || k > n)
+        return PXR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t slots = 0;
+    if (cudaMemcpyAsync(&slots, offsets + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (slots && (!cols || !out_cols)) return PXR_INVALID_ARG;
+    static bool prepared[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (dev >= 0 && dev < 64 && !prepared[dev]) {
+        if (radix_sort_prepare<uint64_t>() != cudaSuccess) return PXR_CUDA_ERROR;
+        prepared[dev] = true;
+    }
+    // the layout of pxr_build_csr for slots / 2 edges: key buffers of `slots` entries
+    const BuildLayout L = build_layout((slots + 1) / 2);
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    uint64_t* k0 = reinterpret_cast<uint64_t*>(base + L.keys0);
+    uint64_t* k1 = reinterpret_cast<uint64_t*>(base + L.keys1);
+    uint32_t* words = reinterpret_cast<uint32_t*>(base + L.words);
+    uint32_t *count = words, *end_bit = words + 2, *err = words + 3, *bad = words + 4;
+    if (cudaMemsetAsync(base + L.hist, 0, L.total - L.hist, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaMemsetAsync(cut_sizes, 0, (size_t)k * 8, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaMemsetAsync(volumes, 0, (size_t)k * 8, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    uint32_t bits = 0;
+    while (bits < 32 && (1ull << bits) < k) ++bits;
+    k_set_u32<<<1, 1, 0, s>>>(end_bit, 32u + bits);
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(((uint64_t)n * 32 + kBuildBlock - 1) / kBuildBlock, 148u * 32u);
+    if (n) k_contract_slots<<<grid, kBuildBlock, 0, s>>>(n, offsets, cols, ids, k,
+                                                         reinterpret_cast<const unsigned long long*>(level_volumes),
+                                                         k0, count, reinterpret_cast<unsigned long long*>(cut_sizes),
+                                                         reinterpret_cast<unsigned long long*>(volumes), bad);
+    SortState st{};
+    st.hist = reinterpret_cast<uint32_t*>(base + L.hist);
+    st.bases = reinterpret_cast<uint32_t*>(base + L.bases);
+    st.pass_info = reinterpret_cast<uint32_t*>(base + L.pass_info);
+    st.tile_ctr = reinterpret_cast<uint32_t*>(base + L.tile_ctr);
+    st.epoch = reinterpret_cast<uint32_t*>(base + L.epoch);
+    st.status = reinterpret_cast<uint64_t*>(base + L.status);
+    st.max_tiles = L.tiles;
+    st.items_moved = nullptr;
+    SortBuffers<uint64_t> b{};
+    b.keys[0] = k0;
+    b.keys[1] = k1;
+    b.count = count;
+    b.end_bit = end_bit;
+    b.capacity = std::max<uint32_t>(slots, 1);
+    if (radix_sort<uint64_t>(b, st, err, s, 64) != cudaSuccess) return PXR_CUDA_ERROR;
+    k_csr_rows<<<grid, kBuildBlock, 0, s>>>(k0, k1, st.pass_info + kMaxPasses, count, k, out_offsets,
+                                            out_cols ? out_cols : reinterpret_cast<uint32_t*>(k1));
+    uint32_t w[5] = {0, 0, 0, 0, 0};
+    if (cudaMemcpyAsync(w, words, 20, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXR_CUDA_ERROR;
+    if (w[4]) return PXR_INVALID_ARG;   // an id outside [0, k) or a column outside [0, n)
+    if (w[3]) return PXR_DEVICE_FAULT;
+    *out_m = w[0] / 2;
+    return PXR_OK;
+}
+
+size_t pxr_contract_scratch_bytes(uint64_t slots) { return build_layout((slots + 1) / 2).total; }
 
 pxr_status pxr_build_csr_finalize(uint32_t n, uint64_t n_edges, const uint32_t* u, const uint32_t* v, void* scratch,
                                   uint32_t* offsets, uint32_t* cols, void* stream) {
