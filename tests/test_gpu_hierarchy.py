@@ -77,3 +77,24 @@ def test_hierarchy_reaches_one_vertex(name):
         if i + 1 < len(levels):
             assert levels[i + 1].m == lvl.cut_edges
         n = lvl.clusters
+
+
+def _ncut(g, labels):
+    src = np.repeat(np.arange(g.n), np.diff(g.offsets.astype(np.int64)))
+    deg = np.diff(g.offsets.astype(np.int64))
+    k = int(labels.max()) + 1
+    cut = np.bincount(labels[src], weights=(labels[src] != labels[g.cols]).astype(np.float64), minlength=k)
+    vol = np.bincount(labels, weights=deg, minlength=k)
+    keep = vol > 0
+    return float(np.sum(cut[keep] / vol[keep]))
+
+
+def test_normalized_cut_finds_the_planted_blocks():
+    from parex_b200.normalized_cut import NormalizedCut
+    g = G.sbm_graph()            # 16 planted blocks
+    levels = H.build(torch.from_numpy(g.offsets.view(np.int32)), torch.from_numpy(g.cols.view(np.int32)))
+    labels = NormalizedCut(levels, g.n).compute(16)
+    assert labels.min() >= 0 and labels.max() <= 16
+    rng = np.random.default_rng(0)
+    random = rng.integers(0, int(labels.max()) + 1, g.n)
+    assert _ncut(g, labels) < 0.25 * _ncut(g, random)
