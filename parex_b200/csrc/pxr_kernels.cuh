@@ -9,6 +9,16 @@
 namespace pxr {
 
 constexpr int kBlock = 256;
+// Walk kernels: CTAs per SM their register budget is sized for, and whether
+// the long-row kernels load the next row's head while gathering this row.
+#ifndef PXR_WALK_PREFETCH
+#define PXR_WALK_PREFETCH 0
+#endif
+#ifdef PXR_WALK_MIN_BLOCKS
+#define PXR_WALK_BOUNDS __launch_bounds__(kBlock, PXR_WALK_MIN_BLOCKS)
+#else
+#define PXR_WALK_BOUNDS __launch_bounds__(kBlock)
+#endif
 constexpr int kScanItems = 8;                        // items per thread in look-back kernels
 constexpr int kScanTile = kBlock * kScanItems;
 // k_relabel runs over the roots, often far fewer than the vertices: smaller
@@ -293,7 +303,7 @@ __device__ __forceinline__ void walk_block_totals(const Dev<OffT>& d, uint32_t v
 }
 
 template <typename OffT, int W>
-__global__ void __launch_bounds__(kBlock) k_walk(Dev<OffT> d, const uint32_t* ids, const float* xt_in,
+__global__ void PXR_WALK_BOUNDS k_walk(Dev<OffT> d, const uint32_t* ids, const float* xt_in,
                                                  float* xt_out) {
     pdl_wait();
     const uint32_t count = d.ctr->n_active;
@@ -1235,8 +1245,29 @@ __device__ __forceinline__ const uint32_t* row_list(const Dev<OffT>& d, int G, u
     return G == 32 ? d.wide : d.heavy;
 }
 
+// A long row's head: vertex, label and slot bounds (label -1 past the list).
+template <typename OffT>
+struct RowHead {
+    uint32_t v;
+    int32_t lab;
+    OffT beg, end;
+};
+
+template <typename OffT>
+__device__ __forceinline__ RowHead<OffT> row_head(const Dev<OffT>& d, const uint32_t* list, uint32_t h, uint32_t cnt) {
+    RowHead<OffT> r{0u, -1, 0, 0};
+    if (h < cnt) {
+        r.v = list[h];
+        r.lab = d.lab[r.v];
+        r.beg = d.off[r.v];
+        r.end = d.off[r.v + 1];
+    }
+    return r;
+}
+
 template <typename OffT, int G>
-__global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* xt_in, float* xt_out) {
+__global__ void PXR_WALK_BOUNDS k_walk_long(Dev<OffT> d, const float* xt_in,
+                                                                          float* xt_out) {
     pdl_wait();
     __shared__ int64_t sh[kBlock / 32];
     const int e = fixed_exponent(d.ctr->xmax_bits, d.nb_bits);
@@ -1246,10 +1277,21 @@ __global__ void __launch_bounds__(kBlock) k_walk_long(Dev<OffT> d, const float* 
     const RowGroups<G> rg;
     uint32_t vmax = 0;
     unsigned long long st_v = 0, st_s = 0, st_g = 0;
+    // With PXR_WALK_PREFETCH the next row's id, label and bounds are loaded
+    // before this row's slots are gathered, so a row's setup loads overlap
+    // the previous row's gathers.
+    RowHead<OffT> nx = row_head(d, list, rg.first, cnt);
     for (uint32_t h = rg.first; h < cnt; h += rg.step) {
-        const uint32_t v = list[h];
-        if (d.lab[v] < 0) continue;
-        const OffT beg = d.off[v], end = d.off[v + 1];
+        RowHead<OffT> cur;
+        if (PXR_WALK_PREFETCH) {
+            cur = nx;
+            nx = row_head(d, list, h + rg.step, cnt);
+        } else {
+            cur = row_head(d, list, h, cnt);
+        }
+        if (cur.lab < 0) continue;
+        const uint32_t v = cur.v;
+        const OffT beg = cur.beg, end = cur.end;
         int64_t acc = 0;
         unsigned long long g = 0;
         for (OffT s = beg + rg.lane; s < end; s += kSlotUnroll * G) {

@@ -114,7 +114,8 @@ LIGHT_DTYPE = np.dtype([("root", "<u4"), ("size", "<u4"), ("origin", "<u4"), ("r
 
 
 def collect_samples(graph, seed: int, sc: float = 0.3, rw: float = 1e-4, device: int = 0,
-                    max_rounds: int = 10000, per_round: int = 20000, sample_seed: int = 0):
+                    max_rounds: int = 10000, per_round: int = 20000, sample_seed: int = 0,
+                    max_samples: int | None = None):
     """Training samples of one plain decomposition, for graphs whose full
     trace would not fit in host memory (the 128^3 grid has up to ~800 k
     clusters per round): the identity (root, size), origin and round of every
@@ -148,7 +149,13 @@ def collect_samples(graph, seed: int, sc: float = 0.3, rw: float = 1e-4, device:
     if not light:
         return np.zeros((0, F), np.float32), np.zeros(0, np.float32)
     t = trace_targets(np.concatenate(light))[np.concatenate(picked)]
-    return np.concatenate(feats), np.log2(1.0 + np.minimum(t, 255)).astype(np.float32)
+    X = np.concatenate(feats)
+    T = np.log2(1.0 + np.minimum(t, 255)).astype(np.float32)
+    if max_samples is not None and X.shape[0] > max_samples:
+        # every trace weighs about the same in training, however many clusters its graph has
+        keep = np.sort(rng.choice(X.shape[0], max_samples, replace=False))
+        X, T = X[keep], T[keep]
+    return X, T
 
 
 def trace_targets(rec: np.ndarray) -> np.ndarray:
@@ -359,6 +366,7 @@ def main(argv=None) -> int:
     t.add_argument("--max-skip", type=int, default=16)
     t.add_argument("--report", default=None)
     t.add_argument("--per-round", type=int, default=20000, help="swept clusters sampled per round of a trace")
+    t.add_argument("--per-trace", type=int, default=60000, help="samples kept per trace (balances the graphs)")
     e = sub.add_parser("eval")
     e.add_argument("--model", default=DEFAULT_MODEL)
     e.add_argument("--safety", type=float, nargs="*", default=[0.25])
@@ -372,7 +380,8 @@ def main(argv=None) -> int:
         for name, make, walk_seed, seeds in TRAIN_GRAPHS:
             for s in seeds:
                 t0 = time.perf_counter()
-                X1, T1 = collect_samples(make(s), seed=walk_seed(s), per_round=args.per_round)
+                X1, T1 = collect_samples(make(s), seed=walk_seed(s), per_round=args.per_round,
+                                         max_samples=args.per_trace)
                 xs.append(X1)
                 ts.append(T1)
                 log(f"trace {name} seed {s}: {X1.shape[0]} samples, {time.perf_counter() - t0:.1f} s")
@@ -381,6 +390,7 @@ def main(argv=None) -> int:
         model = train(X, T, epochs=args.epochs, batch=args.batch, lr=args.lr, over=args.over, log=log)
         model.meta["train_graphs"] = [[n, s, walk_seed(s)] for n, _, walk_seed, ss in TRAIN_GRAPHS for s in ss]
         model.meta["per_round"] = args.per_round
+        model.meta["per_trace"] = args.per_trace
         model.save(args.out)
         report["train"] = model.meta
         if args.eval:
