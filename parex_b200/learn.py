@@ -158,6 +158,25 @@ def collect_samples(graph, seed: int, sc: float = 0.3, rw: float = 1e-4, device:
     return X, T
 
 
+def balance_configs(groups: dict, balance: bool, seed: int = 0):
+    """Concatenate the samples of every configuration; with ``balance`` each
+    configuration is resampled (with replacement) to the size of the largest,
+    so that a small graph's clusters weigh as much as a large graph's."""
+    rng = np.random.default_rng(seed)
+    xs, ts = [], []
+    sizes = {k: sum(x.shape[0] for x, _ in v) for k, v in groups.items()}
+    target = max(sizes.values()) if sizes else 0
+    for name, parts in groups.items():
+        X = np.concatenate([x for x, _ in parts])
+        T = np.concatenate([t for _, t in parts])
+        if balance and 0 < X.shape[0] < target:
+            pick = np.concatenate([np.arange(X.shape[0]), rng.integers(0, X.shape[0], target - X.shape[0])])
+            X, T = X[pick], T[pick]
+        xs.append(X)
+        ts.append(T)
+    return np.concatenate(xs), np.concatenate(ts)
+
+
 def trace_targets(rec: np.ndarray) -> np.ndarray:
     """Safe skips of every record: the number of following rounds in which the
     same vertex set (same root and size) was swept without being cut or
@@ -367,6 +386,7 @@ def main(argv=None) -> int:
     t.add_argument("--report", default=None)
     t.add_argument("--per-round", type=int, default=20000, help="swept clusters sampled per round of a trace")
     t.add_argument("--per-trace", type=int, default=60000, help="samples kept per trace (balances the graphs)")
+    t.add_argument("--balance", action="store_true", help="resample every configuration to the same size")
     e = sub.add_parser("eval")
     e.add_argument("--model", default=DEFAULT_MODEL)
     e.add_argument("--safety", type=float, nargs="*", default=[0.25])
@@ -376,21 +396,21 @@ def main(argv=None) -> int:
     log = lambda s: print(s, file=sys.stderr, flush=True)
     report = {}
     if args.cmd == "train":
-        xs, ts = [], []
+        groups = {}
         for name, make, walk_seed, seeds in TRAIN_GRAPHS:
             for s in seeds:
                 t0 = time.perf_counter()
                 X1, T1 = collect_samples(make(s), seed=walk_seed(s), per_round=args.per_round,
                                          max_samples=args.per_trace)
-                xs.append(X1)
-                ts.append(T1)
+                groups.setdefault(name, []).append((X1, T1))
                 log(f"trace {name} seed {s}: {X1.shape[0]} samples, {time.perf_counter() - t0:.1f} s")
-        X, T = np.concatenate(xs), np.concatenate(ts)
+        X, T = balance_configs(groups, args.balance)
         log(f"dataset: {X.shape[0]} samples, mean target {T.mean():.3f}")
         model = train(X, T, epochs=args.epochs, batch=args.batch, lr=args.lr, over=args.over, log=log)
         model.meta["train_graphs"] = [[n, s, walk_seed(s)] for n, _, walk_seed, ss in TRAIN_GRAPHS for s in ss]
         model.meta["per_round"] = args.per_round
         model.meta["per_trace"] = args.per_trace
+        model.meta["balanced"] = bool(args.balance)
         model.save(args.out)
         report["train"] = model.meta
         if args.eval:
