@@ -223,6 +223,32 @@ def run_reference_cpu(offsets, cols, reps: int, warm=None, warmups: int = 0, tim
     return {"kind": "port", "secs": secs}
 
 
+def run_reference_gpu(offsets, cols, off64, timeout=900):
+    """The reference's own GPU decomposition of the same graph on the same
+    B200 (oracle/_ref/ref_gpu, built from the reference's cuda/ sources with
+    its own flags): CudaDeviceManager::expanderDecomposition timed with CUDA
+    events, one run, for context beside the product's numbers."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "ref_gpu")
+    if not os.path.exists(binary):
+        return {"unavailable": "oracle/_ref/ref_gpu not built"}
+    if off64:
+        return {"unavailable": "the reference's EdgeIx is 32-bit"}
+    with tempfile.TemporaryDirectory() as td:
+        gp = os.path.join(td, "g.pxg")
+        _write_pxg(gp, np.asarray(offsets), np.asarray(cols))
+        try:
+            out = subprocess.run([binary, "time", gp, str(WALK_SEED), str(SC), str(RW), "1"], capture_output=True,
+                                 text=True, timeout=timeout).stdout
+        except subprocess.TimeoutExpired:
+            return {"unavailable": f"did not finish within {timeout} s"}
+    runs = [json.loads(l) for l in out.splitlines() if l.startswith("{")]
+    if not runs:
+        return {"unavailable": "no timing printed"}
+    r = runs[0]
+    return {"loop_ms": r["loop_ms"], "e2e_ms": r["e2e_ms"], "clusters": r["num_clusters_fp"],
+            "edges_per_s": r["m"] / (r["loop_ms"] / 1e3)}
+
+
 def host_graph(name):
     """The workload's CSR on the host, built without the product library
     (the R-MAT graphs by the oracle's C builder, the same edges as the device
@@ -566,6 +592,9 @@ def product_arm(args, rank, world, local_rank):
         extra["cut_edges_learned_over_plain"] = l["cut_edges"] / max(p["cut_edges"], 1)
         extra["every_cluster_certified"] = bool(p["certificate"]["ok"] and l["certificate"]["ok"])
 
+    if world == 1 and not args.no_reference_gpu:
+        extra["reference_gpu"] = run_reference_gpu(off_hn, cols_hn, off64)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         sample, what = cpu_sample(args.workload)
@@ -597,6 +626,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU decomposition of the graph")
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
     ap.add_argument("--schedule", default="both", choices=["both", "plain", "learned"])
     ap.add_argument("--no-connectivity", dest="connectivity", action="store_false",
