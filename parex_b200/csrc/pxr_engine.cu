@@ -700,8 +700,9 @@ cudaError_t op_sweep(pxr_handle* h) {
         phase(h, kPhEmit, 1, [&] {
             launch_pdl(k_emit_sched<OffT>, tiles, kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
         });
-        phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
+        phase(h, kPhNodeDiff, 2 + long_launches(h), [&] {
             launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->vals[0], 1);
+            launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur], 0);
             PXR_LONG(h, k_nodediff_long, d);
         });
     } else {

@@ -363,13 +363,25 @@ __global__ void PXR_WALK_BOUNDS k_walk(Dev<OffT> d, const uint32_t* ids, const f
 // edge differences (nodeDiffKernel_Sparse_WarpParallel, cuda/devSweepCut.h:20-112):
 // +1 per valid neighbour after v in (potential, id) order, -1 per neighbour before.
 
+// A sweep set at most 1 / kSweepListShare of the active list is walked as a list.
+constexpr uint32_t kSweepListShare = 8;
+
 // ids: the active list in vertex order (count n_active), or with sweep_list
 // the sweep set as the learned schedule's emit compacted it (count n_sweep,
 // every entry swept).
+//
+// The learned schedule launches both forms; one returns at once: the sweep
+// set (in the last sort's order, so its rows are scattered) when it is a
+// small part of the active list, the vertex-order scan (coalesced) when it
+// holds a large cluster.
 template <typename OffT, int W>
 __global__ void __launch_bounds__(kBlock) k_nodediff(Dev<OffT> d, const uint32_t* ids, int sweep_list = 0) {
     pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
+    if (d.sched) {
+        const bool small = (uint64_t)d.ctr->n_sweep * kSweepListShare <= d.ctr->n_active;
+        if (sweep_list ? !small : small) return;
+    }
     const uint32_t count = sweep_list ? d.ctr->n_sweep : d.ctr->n_active;
     const uint32_t gl = threadIdx.x & (W - 1);
     const uint32_t groups = (gridDim.x * blockDim.x) / W;
