@@ -1,6 +1,6 @@
 """ctypes loader for libparex_b200.so (the C ABI of include/parex_b200.h).
 
-The library is built in-tree by ``parex_b200/build.py``; there is no CPU
+The library is built in-tree by ``make -C parex_b200/csrc`` (``__graft_entry__.build()``); there is no CPU
 fallback, so a missing or unloadable library raises ImportError.
 """
 from __future__ import annotations
@@ -136,7 +136,7 @@ def load() -> C.CDLL:
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing; build it with parex_b200.build.build()")
+        raise ImportError(f"{LIB_PATH} is missing; build it with make -C parex_b200/csrc (or __graft_entry__.build())")
     L = C.CDLL(LIB_PATH)
     p = C.c_void_p
     u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
