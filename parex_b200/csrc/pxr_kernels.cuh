@@ -1258,6 +1258,33 @@ struct RowGroups {
     }
 };
 
+// Rows of a long-row list that pass `pred`, each handed to `body` with the
+// whole group.  A warp-per-row group tests a window of 32 rows at once, one
+// per lane, and then works the passing rows one after another: lists whose
+// rows mostly fail (clusters not split, not swept) cost one load chain per
+// 32 rows instead of per row.  pred(v) runs per lane; body(v) on every lane.
+template <int G, class Pred, class Body>
+__device__ __forceinline__ void for_each_row(const uint32_t* list, uint32_t cnt, const RowGroups<G>& rg, Pred pred,
+                                             Body body) {
+    if constexpr (G == 32) {
+        for (uint32_t h0 = rg.first * 32u; h0 < cnt; h0 += rg.step * 32u) {
+            const uint32_t h = h0 + rg.lane;
+            const uint32_t v = h < cnt ? list[h] : 0u;
+            uint32_t pass = __ballot_sync(0xFFFFFFFFu, h < cnt && pred(v));
+            while (pass) {
+                const int src = __ffs(pass) - 1;
+                pass &= pass - 1u;
+                body(__shfl_sync(0xFFFFFFFFu, v, src));
+            }
+        }
+    } else {
+        for (uint32_t h = rg.first; h < cnt; h += rg.step) {
+            const uint32_t v = list[h];
+            if (pred(v)) body(v);
+        }
+    }
+}
+
 template <typename OffT>
 __device__ __forceinline__ const uint32_t* row_list(const Dev<OffT>& d, int G, uint32_t* count) {
     *count = G == 32 ? d.n_wide : d.n_heavy;
@@ -1350,11 +1377,11 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
     uint32_t cnt;
     const uint32_t* list = row_list(d, G, &cnt);
     const RowGroups<G> rg;
-    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
-        const uint32_t v = list[h];
+    auto swept = [&](uint32_t v) {
         const int32_t lv = d.lab[v];
-        if (lv < 0) continue;
-        if (d.sched && !(d.sflag[lv] & 2u)) continue;
+        return lv >= 0 && (!d.sched || (d.sflag[lv] & 2u));
+    };
+    for_each_row<G>(list, cnt, rg, swept, [&](uint32_t v) {
         const uint32_t mine = ordered_bits(d.x[v]);
         const OffT beg = d.off[v], end = d.off[v + 1];
         int32_t c = 0;
@@ -1374,7 +1401,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
         }
         c = group_sum<G, int32_t>(c, sh);
         if (rg.lane == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
-    }
+    });
 }
 
 template <typename OffT, int G>
@@ -1385,22 +1412,24 @@ __global__ void __launch_bounds__(kBlock) k_union_long(Dev<OffT> d) {
     uint32_t cnt;
     const uint32_t* list = row_list(d, G, &cnt);
     const RowGroups<G> rg;
-    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
-        const uint32_t v = list[h];
+    auto in_split_cluster = [&](uint32_t v) {
         const int32_t lv = d.lab[v];
-        if (lv < 0) continue;
+        if (lv < 0) return false;
         const uint32_t c = (uint32_t)lv >= k ? (uint32_t)lv - k : (uint32_t)lv;   // cut labels are c or K + c
-        if (c >= k || !d.split[c]) continue;
+        return c < k && d.split[c] != 0;
+    };
+    for_each_row<G>(list, cnt, rg, in_split_cluster, [&](uint32_t v) {
+        const int32_t lv = d.lab[v];
         const OffT beg = d.off[v], end = d.off[v + 1];
         uint32_t hint;
-        if (union_skip_row(d, k, v, lv, hint)) continue;
+        if (union_skip_row(d, k, v, lv, hint)) return;
         for (OffT s = beg + rg.lane; s < end; s += G) {
             const uint32_t nb = d.cols[s];
             if (!slot_valid(nb) || nb == v) continue;
             if (!d.union_sampled && nb > v) break;
             if (d.lab[nb] == lv) uf_join(d.parent, &d.ctr->err, v, nb, hint);
         }
-    }
+    });
 }
 
 template <typename OffT, int G>
@@ -1412,11 +1441,13 @@ __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt,
     const uint32_t* list = row_list(d, G, &cnt);
     const RowGroups<G> rg;
     uint32_t vmax = 0;
-    for (uint32_t h = rg.first; h < cnt; h += rg.step) {
-        const uint32_t v = list[h];
+    // rows of clusters born from a split only: k_ids_disable refreshed x / degree of the others
+    auto rescanned = [&](uint32_t v) {
         const int32_t lv = d.lab[v];
-        if (lv < 0) continue;
-        if (d.nflag[lv] != kRowsScan) continue;   // not split: k_ids_disable refreshed x / degree
+        return lv >= 0 && d.nflag[lv] == kRowsScan;
+    };
+    for_each_row<G>(list, cnt, rg, rescanned, [&](uint32_t v) {
+        const int32_t lv = d.lab[v];
         const OffT beg = d.off[v], end = d.off[v + 1];
         uint32_t deg = 0;
         for (OffT s = beg + rg.lane; s < end; s += G) {
@@ -1434,7 +1465,7 @@ __global__ void __launch_bounds__(kBlock) k_disable_long(Dev<OffT> d, float* xt,
             vmax = b > vmax ? b : vmax;
             atomicAdd(&nt.vol[lv], deg);
         }
-    }
+    });
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) vmax = max(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
     if ((threadIdx.x & 31u) == 0 && vmax) atomicMax(&d.ctr->xmax_bits, vmax);
