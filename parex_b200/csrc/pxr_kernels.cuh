@@ -1259,14 +1259,16 @@ struct RowGroups {
 };
 
 // Rows of a long-row list that pass `pred`, each handed to `body` with the
-// whole group.  A warp-per-row group tests a window of 32 rows at once, one
-// per lane, and then works the passing rows one after another: lists whose
-// rows mostly fail (clusters not split, not swept) cost one load chain per
-// 32 rows instead of per row.  pred(v) runs per lane; body(v) on every lane.
+// whole group.  With `windows` a warp-per-row group tests a window of 32
+// rows at once, one per lane, and then works the passing rows one after
+// another: lists whose rows mostly fail (clusters not split, not swept) cost
+// one load chain per 32 rows instead of per row.  Where most rows pass, the
+// row-by-row order spreads the rows over the warps more evenly.  pred(v)
+// runs per lane; body(v) on every lane.
 template <int G, class Pred, class Body>
 __device__ __forceinline__ void for_each_row(const uint32_t* list, uint32_t cnt, const RowGroups<G>& rg, Pred pred,
-                                             Body body) {
-    if constexpr (G == 32) {
+                                             Body body, bool windows = true) {
+    if (G == 32 && windows) {
         for (uint32_t h0 = rg.first * 32u; h0 < cnt; h0 += rg.step * 32u) {
             const uint32_t h = h0 + rg.lane;
             const uint32_t v = h < cnt ? list[h] : 0u;
@@ -1401,7 +1403,7 @@ __global__ void __launch_bounds__(kBlock) k_nodediff_long(Dev<OffT> d) {
         }
         c = group_sum<G, int32_t>(c, sh);
         if (rg.lane == 0) d.dv[v] = make_int2(c, (int)d.ideg[v]);
-    });
+    }, d.sched != 0);   // the plain form takes the edge differences of every row
 }
 
 template <typename OffT, int G>
