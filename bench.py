@@ -55,7 +55,7 @@ METRIC = "decomp edges/s"
 UNIT = "edges/s"
 WALK_SEED, GRAPH_SEED, SC, RW = 6582, 1, 0.3, 1e-4
 L2_FLUSH_BYTES = 256 << 20
-SAFETY, MAX_SKIP = 0.25, 16
+SAFETY, MAX_SKIP, CUT_GATE = 0.25, 16, 0.01
 
 
 WORKLOADS = {
@@ -435,7 +435,8 @@ def product_arm(args, rank, world, local_rank):
         if args.row_plan:
             dmx.set_row_plan(*[int(t) for t in args.row_plan.split(",")])
         if form == "learned":
-            dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=SAFETY, max_skip=MAX_SKIP)
+            dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=SAFETY, max_skip=MAX_SKIP,
+                             cut_gate=args.cut_gate)
         dmx.set_stream(stream.cuda_stream)
         return dmx
 
@@ -583,7 +584,8 @@ def product_arm(args, rank, world, local_rank):
              "parallelism": (f"{world} ranks, instances split by expected edges" if sharded else "replicas"),
              "job_edges_per_step": job_m}
     if model is not None:
-        extra["learned_schedule"] = {"safety": SAFETY, "max_skip": MAX_SKIP, "model": "parex_b200/data/stop_predictor.npz"}
+        extra["learned_schedule"] = {"safety": SAFETY, "max_skip": MAX_SKIP, "cut_gate": args.cut_gate,
+                                     "model": "parex_b200/data/stop_predictor.npz"}
     if sharded:
         extra["shard_instances"] = len(shard)
     if len(forms) == 2:
@@ -632,6 +634,8 @@ def main():
     ap.add_argument("--schedule", default="both", choices=["both", "plain", "learned"])
     ap.add_argument("--no-connectivity", dest="connectivity", action="store_false",
                     help="skip the connectivity part of the certificate check")
+    ap.add_argument("--cut-gate", type=float, default=CUT_GATE,
+                    help="learned form: after a round that cut more than this fraction of its clusters, sweep all")
     ap.add_argument("--row-plan", default=None, help="force lanes_per_row,light_max,wide_max (default: autotuned)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

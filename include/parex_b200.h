@@ -180,7 +180,9 @@ typedef struct {
     uint32_t trace;            /* nonzero: keep one pxr_cluster_record per active cluster per round */
     float safety;              /* fraction of the predicted skips taken                             */
     uint32_t max_skip;         /* cap on consecutive skipped rounds                                 */
-    uint32_t reserved[4];
+    float cut_gate;            /* a round that cuts more than cut_gate x its clusters skips no sweep
+                                  in the next round (every cluster swept, as in PLAIN); 0: off      */
+    uint32_t reserved[3];
 } pxr_schedule;
 
 /* One active cluster after the last round (trace mode).  origin: 1 swept and

@@ -65,6 +65,7 @@ struct RoundCtr {
     uint32_t max_csize_next;  // largest cluster kept for the next round
     uint32_t walk_only;       // learned schedule: no cluster is due this round, only the walk runs
     uint32_t any_split;       // some cluster of this round is split (cut, or all components): union-find runs
+    uint32_t n_cut_swept;     // n_cut of this round's sweep, kept through the cut stage (learned schedule's gate)
     unsigned long long stat_sort_items;     // traffic counters since initialisation (the walk's: kStatSlots)
     unsigned long long stat_sort_passes;
     unsigned long long stat_swept_items;     // sweep input vertices, summed over rounds

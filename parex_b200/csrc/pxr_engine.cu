@@ -518,6 +518,7 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.mlp = h->mlp;
     d.safety = h->sched.safety;
     d.max_skip = h->sched.max_skip;
+    d.cut_gate = h->sched.cut_gate;
     d.records = h->records;
     return d;
 }
@@ -2016,6 +2017,8 @@ pxr_status pxr_set_schedule(pxr_handle* h, const pxr_schedule* cfg, const uint16
         if (!weights || !norm) return fail(h, PXR_INVALID_ARG, "the learned schedule needs weights and norm");
         if (!(cfg->safety >= 0.0f) || cfg->max_skip > 0xFFFFu)
             return fail(h, PXR_INVALID_ARG, "safety must be >= 0 and max_skip below 65536");
+        if (!(cfg->cut_gate >= 0.0f) || !(cfg->cut_gate <= 1.0f))
+            return fail(h, PXR_INVALID_ARG, "cut_gate must lie in [0, 1]");
         std::vector<float> img(kMlpImage);
         for (int p = 0; p < kMlpParams; ++p) {
             const uint32_t b = (uint32_t)weights[p] << 16;

@@ -177,6 +177,7 @@ __global__ void k_round_prep(Dev<OffT> d, int stage, cudaGraphConditionalHandle 
         d.lb_epoch[lane] += 1;
     }
     if (lane != 0) return;
+    if (stage == 2) c->n_cut_swept = c->n_cut;   // the sweep's count, read by the cut stage
     c->n_cut = 0;
     c->n_roots = 0;
     if (stage == 0) {
@@ -975,8 +976,9 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
                 nt.vol[nl] = kind == kOriginChild ? 0u : t.vol[c];
                 if (kind == kOriginCarried) {
                     const uint16_t sk = t.skip[c];
-                    // due next round once its spread is below the threshold (k_due_scan)
-                    nt.skip[nl] = (sk > 0 && !(d.sflag[c] & 4u)) ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+                    // due next round once its spread is below the threshold (k_due_scan),
+                    // or after a round that cut many clusters
+                    nt.skip[nl] = (sk > 0 && !(d.sflag[c] & 4u) && !cut_gate_on(d)) ? (uint16_t)(sk - 1u) : (uint16_t)0u;
                     nt.hist[nl] = t.hist[c];
                 }
             } else {

@@ -76,6 +76,34 @@ __device__ __forceinline__ float mlp_forward(const float* img, const float* f, f
     return y;
 }
 
+// The output of mlp_forward without its intermediates, for inference: the
+// same float operations in the same order (layer-1 neurons summed over the
+// inputs in order; each layer-2 neuron summed over layer 1 in order, then
+// added to the output in neuron order), so the result is bit-identical,
+// with 32 live accumulators instead of 144 stored values.
+__device__ __forceinline__ float mlp_infer(const float* img, const float* f) {
+    float h1[kMlpHidden];
+#pragma unroll
+    for (int o = 0; o < kMlpHidden; ++o) h1[o] = img[kOffB1 + o];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) {
+        const float zi = bf16_round(__fmul_rn(__fsub_rn(f[i], img[kMlpParams + i]), img[kMlpParams + kMlpIn + i]));
+#pragma unroll
+        for (int o = 0; o < kMlpHidden; ++o) h1[o] = __fadd_rn(h1[o], __fmul_rn(img[kOffW1 + o * kMlpIn + i], zi));
+    }
+#pragma unroll
+    for (int o = 0; o < kMlpHidden; ++o) h1[o] = bf16_round(fmaxf(h1[o], 0.0f));
+    float y = img[kOffB3];
+#pragma unroll 1
+    for (int o = 0; o < kMlpHidden; ++o) {
+        float a = img[kOffB2 + o];
+#pragma unroll
+        for (int i = 0; i < kMlpHidden; ++i) a = __fadd_rn(a, __fmul_rn(img[kOffW2 + o * kMlpHidden + i], h1[i]));
+        y = __fadd_rn(y, __fmul_rn(img[kOffW3 + o], bf16_round(fmaxf(a, 0.0f))));
+    }
+    return y;
+}
+
 // Per-cluster features of the schedule (pxr_cluster_record::features).
 // s, vol: size and internal volume; pot: potential spread (max - min); sp:
 // best sweep sparsity this round (2 when none); prev_*: the same at the

@@ -119,6 +119,7 @@ struct Dev {
     LookbackState lb_sched, lb_emit, lb_carry;
     const float* mlp;         // bf16 weights widened to float, then input mean and scale
     float safety;             // skip = floor(safety * (2^y - 1))
+    float cut_gate;           // a round cutting more than cut_gate x its clusters: no skip next round
     uint32_t max_skip;
     void* records;            // pxr_cluster_record[] when trace is on
 };
@@ -144,5 +145,13 @@ enum : int {
 };
 
 __device__ __forceinline__ uint32_t bitlen(uint32_t v) { return v ? 32u - __clz(v) : 0u; }
+
+// Learned schedule: this round cut more than cut_gate x its clusters, so the
+// next round sweeps every cluster (read after the cut, before the round ends).
+template <typename OffT>
+__device__ __forceinline__ bool cut_gate_on(const Dev<OffT>& d) {
+    return d.cut_gate > 0.0f &&
+           __uint2float_rn(d.ctr->n_cut_swept) > __fmul_rn(d.cut_gate, __uint2float_rn(d.ctr->n_clusters));
+}
 
 }  // namespace pxr

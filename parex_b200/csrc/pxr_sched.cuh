@@ -320,8 +320,11 @@ __global__ void __launch_bounds__(kBlock) k_carry_vertices(Dev<OffT> d, ClusterT
 // After the round, per cluster of the next round: features, the sweep
 // history and, in the learned modes, the MLP's skip count.  Carried clusters
 // were already handled by k_relabel (counter decremented, history kept).
+// Inference keeps only the layer-1 activations live (mlp_infer): 128
+// registers with a few spilled, two CTAs per SM (the training forward's
+// 144 stored values held it to one).
 template <typename OffT>
-__global__ void __launch_bounds__(kBlock, 1) k_schedule(Dev<OffT> d, ClusterTables t, ClusterTables nt) {
+__global__ void __launch_bounds__(kBlock, 2) k_schedule(Dev<OffT> d, ClusterTables t, ClusterTables nt) {
     pdl_wait();
     if (d.ctr->walk_only) return;   // nothing due: the round only walks
     __shared__ float img[kMlpImage];
@@ -355,15 +358,15 @@ __global__ void __launch_bounds__(kBlock, 1) k_schedule(Dev<OffT> d, ClusterTabl
         if (kind == kOriginSwept) h = t.hist[c];
         const bool has_prev = kind == kOriginSwept && h.age > 0;
         const uint32_t dr = has_prev ? round - h.round : 0u;
-        float f[kMlpIn];
-        cluster_features(f, size, vol, pot, sp, has_prev, h.pot, h.sp, dr, kind == kOriginSwept ? h.age : 0u, round,
-                         d.rw_threshold, d.sc_threshold);
+        const uint32_t age = kind == kOriginSwept ? h.age : 0u;
         float y = 0.0f;
         uint32_t sk = 0;
         if (d.sched && kind == kOriginSwept) {
-            float z[kMlpIn], a1[kMlpHidden], h1[kMlpHidden], a2[kMlpHidden], h2[kMlpHidden];
-            y = mlp_forward(img, f, z, a1, h1, a2, h2);
-            sk = skip_from_prediction(y, d.safety, d.max_skip);
+            float f[kMlpIn];
+            cluster_features(f, size, vol, pot, sp, has_prev, h.pot, h.sp, dr, age, round, d.rw_threshold,
+                             d.sc_threshold);
+            y = mlp_infer(img, f);
+            sk = cut_gate_on(d) ? 0u : skip_from_prediction(y, d.safety, d.max_skip);
         }
         if (d.sched) nt.skip[nl] = (uint16_t)sk;
         const SchedHist nh{pot, sp, round, kind == kOriginSwept ? h.age + 1u : 0u};
@@ -384,6 +387,10 @@ __global__ void __launch_bounds__(kBlock, 1) k_schedule(Dev<OffT> d, ClusterTabl
             o.skip = sk;
             o.prediction = y;
             o.has_prev = has_prev ? 1u : 0u;
+            // the features again (the same function of the same values): not kept live across the MLP
+            float f[kMlpIn];
+            cluster_features(f, size, vol, pot, sp, has_prev, h.pot, h.sp, dr, age, round, d.rw_threshold,
+                             d.sc_threshold);
 #pragma unroll
             for (int i = 0; i < kMlpIn; ++i) o.features[i] = f[i];
         }

@@ -265,10 +265,12 @@ class CudaDeviceManager:
         return {f: getattr(st, f) for f, _ in _lib.Stats._fields_}
 
     def set_schedule(self, mode: int, weights=None, norm=None, safety: float = 0.5, max_skip: int = 16,
-                     trace: bool = False) -> None:
+                     trace: bool = False, cut_gate: float = 0.0) -> None:
         """Learned sweep schedule (pxr_set_schedule).  weights: MLP_PARAMS bf16
-        bit patterns (uint16); norm: 16 means then 16 scales."""
-        cfg = _lib.Schedule(mode, 1 if trace else 0, safety, max_skip)
+        bit patterns (uint16); norm: 16 means then 16 scales.  cut_gate: after
+        a round that cut more than this fraction of its clusters, the next
+        round sweeps every cluster (0: off)."""
+        cfg = _lib.Schedule(mode, 1 if trace else 0, safety, max_skip, cut_gate)
         w = n = None
         if weights is not None:
             w = np.ascontiguousarray(weights, dtype=np.uint16)

@@ -62,30 +62,40 @@ def test_trace_keeps_plain_result_and_features(name):
     np.testing.assert_array_equal(a.getFinalPartition().clusterIds, b.getFinalPartition().clusterIds)
 
 
+@pytest.mark.parametrize("gate", [0.0, 0.02])
 @pytest.mark.parametrize("name", sorted(GRAPHS))
-def test_scheduled_rounds_match_oracle(name):
+def test_scheduled_rounds_match_oracle(name, gate):
     g = GRAPHS[name]()
     model = _random_model(1)
     dm = P.CudaDeviceManager(driver=P.DRIVER_STREAM)
-    dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=1.0, max_skip=4, trace=True)
+    dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=1.0, max_skip=4, trace=True,
+                    cut_gate=gate)
     dm.initialize(g)
     orc = O.Oracle(g.offsets, g.cols, O.MODE_PXR)
     orc.set_potentials(dm.readRandomWalkValues().astype(np.float64))
     due = np.ones(1, dtype=np.uint8)
     skipped = 0
+    gated_rounds = 0
     for _ in range(500):
         if dm.getNumClusters() == 0:
             break
         assert orc.n_clusters == dm.getNumClusters()
+        k_round = np.float32(dm.getNumClusters())
         orc.scheduled_round(due)
         dm.iterateRandomWalk()
         dm.computeSweepCuts()
+        cut = np.float32(dm.stats()["clusters_with_cut"])   # clusters this round's sweep cuts
         dm.cutClusters()
         np.testing.assert_array_equal(dm.downloadLabels(), orc.labels())
         np.testing.assert_array_equal(_bits(dm.readRandomWalkValues()), _bits(orc.potentials()))
         np.testing.assert_array_equal(dm.downloadDegrees(), orc.internal_degrees())
         np.testing.assert_array_equal(dm.downloadGraph()[1], orc.cols())
         rec = dm.cluster_records()
+        # the cut gate: a round that cut more than gate x its clusters is followed by a full sweep
+        gated = gate > 0 and cut > np.float32(gate) * k_round
+        if gated:
+            assert np.all(rec["skip"] == 0)
+            gated_rounds += 1
         # the product's predictions are the oracle network's on the same features
         sw = rec["origin"] == learn.ORIGIN_SWEPT
         if np.any(sw):
@@ -93,11 +103,14 @@ def test_scheduled_rounds_match_oracle(name):
             np.testing.assert_array_equal(_bits(rec["prediction"][sw]), _bits(y))
             r = np.exp2(np.minimum(y.astype(np.float64), 16.0)) - 1.0
             clear = np.abs(r - np.round(r)) > 1e-4          # away from a rounding boundary of floor()
-            np.testing.assert_array_equal(rec["skip"][sw][clear], M.skip_from_prediction(y, 1.0, 4)[clear])
+            want = np.zeros(int(np.count_nonzero(sw)), dtype=np.int64) if gated else M.skip_from_prediction(y, 1.0, 4)
+            np.testing.assert_array_equal(rec["skip"][sw][clear], want[clear])
         due = (rec["skip"] == 0).astype(np.uint8)
         skipped += int(np.count_nonzero(rec["skip"]))
     assert dm.getNumClusters() == 0
     assert skipped > 0, "the random schedule should skip some sweeps"
+    if gate and name != "rmat11":   # the R-MAT graph's sweeps rarely cut: its rounds stay below the gate
+        assert gated_rounds > 0, "some round should cut more than the gate"
     ids, k = orc.final_partition()
     fp = dm.getFinalPartition()
     np.testing.assert_array_equal(fp.clusterIds, ids)
