@@ -312,6 +312,8 @@ struct pxr_handle {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t side_stream = nullptr;   // captures the bodies of IF nodes
+    cudaStream_t walk_side[2] = {};       // the wide- and heavy-row walk kernels, beside the light-row one
+    cudaEvent_t walk_ev[3] = {};          // fork, and the two joins
     cudaStream_t stream = nullptr;
     bool initialized = false;
     bool off64 = false;
@@ -653,17 +655,54 @@ cudaError_t if_region(pxr_handle* h, cudaGraphConditionalHandle cond, F&& body) 
     return cudaStreamUpdateCaptureDependencies(h->stream, &node, 1, cudaStreamSetCaptureDependencies);
 }
 
+// A row kernel in its three parts, which work disjoint rows: light(st)
+// launches the light-row kernel(s) on s, wide(st) and heavy(st) the
+// warp- and CTA-per-row kernels on the handle's two side streams, forked
+// from s and joined back into it.  Running side by side, each part fills the
+// SMs the others leave idle in their last wave (in a captured graph the three
+// are parallel branches).  With no long rows, light(s) alone.
+template <class Light, class Wide, class Heavy>
+void launch_row_parts(pxr_handle* h, cudaStream_t s, Light light, Wide wide, Heavy heavy) {
+    if (!h->n_wide && !h->n_heavy) {
+        light(s);
+        return;
+    }
+    cudaEventRecord(h->walk_ev[0], s);
+    if (h->n_wide) {
+        cudaStreamWaitEvent(h->walk_side[0], h->walk_ev[0], 0);
+        wide(h->walk_side[0]);
+        cudaEventRecord(h->walk_ev[1], h->walk_side[0]);
+    }
+    if (h->n_heavy) {
+        cudaStreamWaitEvent(h->walk_side[1], h->walk_ev[0], 0);
+        heavy(h->walk_side[1]);
+        cudaEventRecord(h->walk_ev[2], h->walk_side[1]);
+    }
+    light(s);
+    if (h->n_wide) cudaStreamWaitEvent(s, h->walk_ev[1], 0);
+    if (h->n_heavy) cudaStreamWaitEvent(s, h->walk_ev[2], 0);
+}
+
+// One walk step: light rows of the active list (W lanes each), the wide list
+// (a warp per row) and the heavy list (a CTA per row).
+template <typename OffT, int W>
+void launch_walk(pxr_handle* h, const Dev<OffT>& d, cudaStream_t s, const float* xt_in, float* xt_out) {
+    launch_row_parts(
+        h, s,
+        [&](cudaStream_t st) {
+            k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, st>>>(d, h->ids[h->acur], xt_in, xt_out);
+        },
+        [&](cudaStream_t st) { k_walk_long<OffT, 32><<<wide_grid(h), kBlock, 0, st>>>(d, xt_in, xt_out); },
+        [&](cudaStream_t st) { k_walk_long<OffT, kBlock><<<heavy_grid(h), kBlock, 0, st>>>(d, xt_in, xt_out); });
+}
+
 template <typename OffT, int W>
 cudaError_t op_walk(pxr_handle* h, bool in_round = false) {
     Dev<OffT> d = make_dev<OffT>(h);
     cudaStream_t s = h->stream;
     hold_for_profiling(h);
     phase(h, kPhBook, 1, [&] { launch_pdl(k_round_prep<OffT>, 1, 32, 0, s, d, 0, kNoCond, kNoCond); });
-    phase(h, kPhWalk, 1 + long_launches(h), [&] {
-        launch_pdl(k_walk<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur], h->xt[h->xcur],
-                                                                          h->xt[h->xcur ^ 1]);
-        PXR_LONG(h, k_walk_long, d, h->xt[h->xcur], h->xt[h->xcur ^ 1]);
-    });
+    phase(h, kPhWalk, 1 + long_launches(h), [&] { launch_walk<OffT, W>(h, d, s, h->xt[h->xcur], h->xt[h->xcur ^ 1]); });
     // the next walk's fixed-point scale follows max |x'|; inside a plain round
     // the cut stage recomputes it over the recentred potentials anyway
     if (!in_round || h->sched.mode) phase(h, kPhBook, 1, [&] { launch_pdl(k_after_walk<OffT>, 1, 1, 0, s, d); });
@@ -702,14 +741,24 @@ cudaError_t op_sweep(pxr_handle* h) {
             launch_pdl(k_emit_sched<OffT>, tiles, kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
         });
         phase(h, kPhNodeDiff, 2 + long_launches(h), [&] {
-            launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->vals[0], 1);
-            launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur], 0);
-            PXR_LONG(h, k_nodediff_long, d);
+            launch_row_parts(
+                h, s,
+                [&](cudaStream_t st) {
+                    k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, st>>>(d, h->vals[0], 1);
+                    k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, st>>>(d, h->ids[h->acur], 0);
+                },
+                [&](cudaStream_t st) { k_nodediff_long<OffT, 32><<<wide_grid(h), kBlock, 0, st>>>(d); },
+                [&](cudaStream_t st) { k_nodediff_long<OffT, kBlock><<<heavy_grid(h), kBlock, 0, st>>>(d); });
         });
     } else {
         phase(h, kPhNodeDiff, 1 + long_launches(h), [&] {
-            launch_pdl(k_nodediff<OffT, W>, grid_for((uint64_t)h->n * W), kBlock, 0, s, d, h->ids[h->acur], 0);
-            PXR_LONG(h, k_nodediff_long, d);
+            launch_row_parts(
+                h, s,
+                [&](cudaStream_t st) {
+                    k_nodediff<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, st>>>(d, h->ids[h->acur], 0);
+                },
+                [&](cudaStream_t st) { k_nodediff_long<OffT, 32><<<wide_grid(h), kBlock, 0, st>>>(d); },
+                [&](cudaStream_t st) { k_nodediff_long<OffT, kBlock><<<heavy_grid(h), kBlock, 0, st>>>(d); });
         });
         phase(h, kPhEmit, 1, [&] {
             launch_pdl(k_emit<OffT>, grid_for(h->n), kBlock, 0, s, d, h->act[h->acur], h->keys[0], h->vals[0], t.best);
@@ -1110,9 +1159,7 @@ std::map<std::vector<uint64_t>, RowPlan> g_plan_cache;
 
 template <typename OffT, int W>
 cudaError_t probe_walk(pxr_handle* h, Dev<OffT> d, float* xt_out) {
-    cudaStream_t s = h->stream;
-    k_walk<OffT, W><<<grid_for((uint64_t)h->n * W), kBlock, 0, s>>>(d, h->ids[h->acur], h->xt[h->xcur], xt_out);
-    PXR_LONG(h, k_walk_long, d, h->xt[h->xcur], xt_out);
+    launch_walk<OffT, W>(h, d, h->stream, h->xt[h->xcur], xt_out);
     return cudaGetLastError();
 }
 
@@ -1511,6 +1558,11 @@ pxr_status pxr_create(const pxr_config* cfg, pxr_handle** out) {
     if (cudaSetDevice(h->device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->walk_side[0], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->walk_side[1], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->walk_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->walk_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->walk_ev[2], cudaEventDisableTiming) != cudaSuccess ||
         cudaMallocHost(&h->h_ctr, sizeof(RoundCtr)) != cudaSuccess) {
         delete h;
         return PXR_CUDA_ERROR;
@@ -1539,6 +1591,10 @@ void pxr_destroy(pxr_handle* h) {
     if (h->h_ctr) cudaFreeHost(h->h_ctr);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     if (h->side_stream) cudaStreamDestroy(h->side_stream);
+    for (cudaStream_t st : h->walk_side)
+        if (st) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : h->walk_ev)
+        if (ev) cudaEventDestroy(ev);
     delete h;
 }
 
