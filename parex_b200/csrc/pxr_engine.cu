@@ -831,8 +831,14 @@ cudaError_t op_cut(pxr_handle* h) {
             launch_pdl(k_compress<OffT>, grid_for(h->n), kBlock, 0, s, d, h->ids[h->acur]);
             launch_pdl(k_union_reps<OffT>, grid_for(h->n), kBlock, 0, s, d, t, h->vals[0], h->vals[1]);
         }
-        launch_pdl(k_union<OffT, kUnionLanes>, grid_for((uint64_t)h->n * kUnionLanes), kBlock, 0, s, d, h->ids[h->acur]);
-        PXR_LONG(h, k_union_long, d);
+        // lock-free unions over disjoint rows: the three parts side by side
+        launch_row_parts(
+            h, s,
+            [&](cudaStream_t st) {
+                k_union<OffT, kUnionLanes><<<grid_for((uint64_t)h->n * kUnionLanes), kBlock, 0, st>>>(d, h->ids[h->acur]);
+            },
+            [&](cudaStream_t st) { k_union_long<OffT, 32><<<wide_grid(h), kBlock, 0, st>>>(d); },
+            [&](cudaStream_t st) { k_union_long<OffT, kBlock><<<heavy_grid(h), kBlock, 0, st>>>(d); });
     });
     phase(h, kPhComponents, 1, [&] {
         launch_pdl(k_components_data<OffT>, std::min(tiles, kMaxGrid), kBlock, 0, s, d, t, h->vals[0], h->vals[1],
@@ -853,8 +859,14 @@ cudaError_t op_cut(pxr_handle* h) {
                                                h->act[h->acur ^ 1], h->par[h->acur ^ 1]);
     });
     phase(h, kPhDisable, 1 + long_launches(h), [&] {
-        launch_pdl(k_ids_disable<OffT, W>, tiles, kBlock, 0, s, d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
-        PXR_LONG(h, k_disable_long, d, h->xt[h->xcur], nt);
+        // disjoint rows; shared results are atomics (volumes, max |x|): side by side
+        launch_row_parts(
+            h, s,
+            [&](cudaStream_t st) {
+                k_ids_disable<OffT, W><<<tiles, kBlock, 0, st>>>(d, h->ids[h->acur], h->ids[h->acur ^ 1], h->xt[h->xcur], nt);
+            },
+            [&](cudaStream_t st) { k_disable_long<OffT, 32><<<wide_grid(h), kBlock, 0, st>>>(d, h->xt[h->xcur], nt); },
+            [&](cudaStream_t st) { k_disable_long<OffT, kBlock><<<heavy_grid(h), kBlock, 0, st>>>(d, h->xt[h->xcur], nt); });
     });
     phase(h, kPhCvol, 1, [&] { launch_pdl(k_cvol_scan<OffT>, tiles, kBlock, 0, s, d, nt); });
     if (h->sched.mode || d.trace)
