@@ -55,7 +55,7 @@ METRIC = "decomp edges/s"
 UNIT = "edges/s"
 WALK_SEED, GRAPH_SEED, SC, RW = 6582, 1, 0.3, 1e-4
 L2_FLUSH_BYTES = 256 << 20
-SAFETY, MAX_SKIP, CUT_GATE = 0.25, 16, 0.01
+SAFETY, MAX_SKIP, CUT_GATE, DUE_PERIOD = 0.25, 16, 0.01, 8
 
 
 WORKLOADS = {
@@ -436,7 +436,7 @@ def product_arm(args, rank, world, local_rank):
             dmx.set_row_plan(*[int(t) for t in args.row_plan.split(",")])
         if form == "learned":
             dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=SAFETY, max_skip=MAX_SKIP,
-                             cut_gate=args.cut_gate)
+                             cut_gate=args.cut_gate, due_period=args.due_period)
         dmx.set_stream(stream.cuda_stream)
         return dmx
 
@@ -585,6 +585,7 @@ def product_arm(args, rank, world, local_rank):
              "job_edges_per_step": job_m}
     if model is not None:
         extra["learned_schedule"] = {"safety": SAFETY, "max_skip": MAX_SKIP, "cut_gate": args.cut_gate,
+                                     "due_period": args.due_period,
                                      "model": "parex_b200/data/stop_predictor.npz"}
     if sharded:
         extra["shard_instances"] = len(shard)
@@ -636,6 +637,8 @@ def main():
                     help="skip the connectivity part of the certificate check")
     ap.add_argument("--cut-gate", type=float, default=CUT_GATE,
                     help="learned form: after a round that cut more than this fraction of its clusters, sweep all")
+    ap.add_argument("--due-period", type=int, default=DUE_PERIOD,
+                    help="learned form: clusters come due only in rounds whose index is a multiple of this")
     ap.add_argument("--row-plan", default=None, help="force lanes_per_row,light_max,wide_max (default: autotuned)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -87,7 +87,7 @@ SCHEDULE_PLAIN, SCHEDULE_LEARNED, SCHEDULE_AUDIT = 0, 1, 2
 
 class Schedule(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("trace", C.c_uint32), ("safety", C.c_float), ("max_skip", C.c_uint32),
-                ("cut_gate", C.c_float), ("reserved", C.c_uint32 * 3)]
+                ("cut_gate", C.c_float), ("due_period", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 class ClusterRecord(C.Structure):

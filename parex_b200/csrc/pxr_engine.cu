@@ -521,6 +521,7 @@ Dev<OffT> make_dev(pxr_handle* h) {
     d.safety = h->sched.safety;
     d.max_skip = h->sched.max_skip;
     d.cut_gate = h->sched.cut_gate;
+    d.due_period = h->sched.due_period;
     d.records = h->records;
     return d;
 }
@@ -2087,6 +2088,7 @@ pxr_status pxr_set_schedule(pxr_handle* h, const pxr_schedule* cfg, const uint16
             return fail(h, PXR_INVALID_ARG, "safety must be >= 0 and max_skip below 65536");
         if (!(cfg->cut_gate >= 0.0f) || !(cfg->cut_gate <= 1.0f))
             return fail(h, PXR_INVALID_ARG, "cut_gate must lie in [0, 1]");
+        if (cfg->due_period > 1024u) return fail(h, PXR_INVALID_ARG, "due_period must be at most 1024");
         std::vector<float> img(kMlpImage);
         for (int p = 0; p < kMlpParams; ++p) {
             const uint32_t b = (uint32_t)weights[p] << 16;

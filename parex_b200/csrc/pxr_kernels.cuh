@@ -978,7 +978,7 @@ __global__ void __launch_bounds__(kBlock) k_relabel(Dev<OffT> d, const uint32_t*
                     const uint16_t sk = t.skip[c];
                     // due next round once its spread is below the threshold (k_due_scan),
                     // or after a round that cut many clusters
-                    nt.skip[nl] = (sk > 0 && !(d.sflag[c] & 4u) && !cut_gate_on(d)) ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+                    nt.skip[nl] = due_aligned(d, (sk > 0 && !(d.sflag[c] & 4u) && !cut_gate_on(d)) ? sk - 1u : 0u, cnt);
                     nt.hist[nl] = t.hist[c];
                 }
             } else {

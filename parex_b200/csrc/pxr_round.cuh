@@ -120,6 +120,7 @@ struct Dev {
     const float* mlp;         // bf16 weights widened to float, then input mean and scale
     float safety;             // skip = floor(safety * (2^y - 1))
     float cut_gate;           // a round cutting more than cut_gate x its clusters: no skip next round
+    uint32_t due_period;      // > 1: clusters come due only in rounds whose index is a multiple of it
     uint32_t max_skip;
     void* records;            // pxr_cluster_record[] when trace is on
 };
@@ -152,6 +153,25 @@ template <typename OffT>
 __device__ __forceinline__ bool cut_gate_on(const Dev<OffT>& d) {
     return d.cut_gate > 0.0f &&
            __uint2float_rn(d.ctr->n_cut_swept) > __fmul_rn(d.cut_gate, __uint2float_rn(d.ctr->n_clusters));
+}
+
+// Learned schedule: the next round's skip sk of a cluster of `size`
+// vertices.  A small cluster (under 1/kDueSmallShare of the active vertices)
+// is held at 1 while the next round's index is not a multiple of
+// due_period: the sweeps of small clusters, which each cost a round its
+// passes over every active vertex, gather into fewer rounds and the rest
+// only walk.  Larger clusters keep their own timing (holding them back lets
+// the walk mix past cuts they would have made); after a gated round every
+// cluster stays due.
+constexpr uint32_t kDueSmallShare = 1024;
+
+template <typename OffT>
+__device__ __forceinline__ uint16_t due_aligned(const Dev<OffT>& d, uint32_t sk, uint32_t size) {
+    const uint32_t P = d.due_period;
+    if (sk == 0 && P > 1 && (d.ctr->rounds + 1u) % P != 0u && (uint64_t)size * kDueSmallShare < d.ctr->n_active &&
+        !cut_gate_on(d))
+        return 1u;
+    return (uint16_t)sk;
 }
 
 }  // namespace pxr

@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kBlock) k_carry_all(Dev<OffT> d, ClusterTables
         nt.root[c] = t.root[c];
         nt.best[c] = ~0ull;
         const uint16_t sk = t.skip[c];
-        nt.skip[c] = (sk > 0 && !(d.sflag[c] & 4u)) ? (uint16_t)(sk - 1u) : (uint16_t)0u;
+        nt.skip[c] = due_aligned(d, (sk > 0 && !(d.sflag[c] & 4u)) ? sk - 1u : 0u, t.size[c]);
         nt.hist[c] = t.hist[c];
         if (d.trace) {
             pxr_cluster_record& o = static_cast<pxr_cluster_record*>(d.records)[c];
@@ -368,7 +368,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_schedule(Dev<OffT> d, ClusterTabl
             y = mlp_infer(img, f);
             sk = cut_gate_on(d) ? 0u : skip_from_prediction(y, d.safety, d.max_skip);
         }
-        if (d.sched) nt.skip[nl] = (uint16_t)sk;
+        if (d.sched) {
+            sk = due_aligned(d, sk, size);
+            nt.skip[nl] = (uint16_t)sk;
+        }
         const SchedHist nh{pot, sp, round, kind == kOriginSwept ? h.age + 1u : 0u};
         nt.hist[nl] = nh;
         if (d.trace) {

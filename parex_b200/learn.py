@@ -306,11 +306,12 @@ def cut_edges(graph, ids: np.ndarray) -> int:
 
 def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, max_skip: int, device: int = 0,
              reps: int = 1, driver: int = _lib.DRIVER_GRAPH, sc: float = 0.3, rw: float = 1e-4,
-             cut_gate: float = 0.01) -> dict:
+             cut_gate: float = 0.01, due_period: int = 8) -> dict:
     import torch
     dm = CudaDeviceManager(seed=seed, sc_threshold=sc, rw_threshold=rw, device=device, driver=driver)
     if mode != _lib.SCHEDULE_PLAIN:
-        dm.set_schedule(mode, model.weights, model.norm, safety=safety, max_skip=max_skip, cut_gate=cut_gate)
+        dm.set_schedule(mode, model.weights, model.norm, safety=safety, max_skip=max_skip, cut_gate=cut_gate,
+                        due_period=due_period)
     times = []
     rounds = 0
     for _ in range(reps):
@@ -330,19 +331,22 @@ def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, ma
 
 
 def compare(graph, model: Model, seed: int = 6582, safety: float = 0.25, max_skip: int = 16, device: int = 0,
-            reps: int = 3, audit: bool = True, cut_gate: float = 0.01, plain: dict | None = None) -> dict:
+            reps: int = 3, audit: bool = True, cut_gate: float = 0.01, plain: dict | None = None,
+            due_period: int = 8) -> dict:
     if plain is None:
         plain = run_mode(graph, _lib.SCHEDULE_PLAIN, None, seed, safety, max_skip, device, reps)
-    learned = run_mode(graph, _lib.SCHEDULE_LEARNED, model, seed, safety, max_skip, device, reps, cut_gate=cut_gate)
+    learned = run_mode(graph, _lib.SCHEDULE_LEARNED, model, seed, safety, max_skip, device, reps, cut_gate=cut_gate,
+                       due_period=due_period)
     res = {"graph": graph.name, "n": graph.n, "m": graph.m, "safety": safety, "max_skip": max_skip,
-           "cut_gate": cut_gate,
+           "cut_gate": cut_gate, "due_period": due_period,
            "plain": {k: v for k, v in plain.items() if k != "ids"},
            "learned": {k: v for k, v in learned.items() if k != "ids"}}
     res["speedup"] = plain["ms"] / learned["ms"] if learned["ms"] > 0 else None
     res["cut_ratio"] = learned["cut_edges"] / max(plain["cut_edges"], 1)
     res["swept_ratio"] = learned["swept_items"] / max(plain["swept_items"], 1)
     if audit:
-        aud = run_mode(graph, _lib.SCHEDULE_AUDIT, model, seed, safety, max_skip, device, 1, cut_gate=cut_gate)
+        aud = run_mode(graph, _lib.SCHEDULE_AUDIT, model, seed, safety, max_skip, device, 1, cut_gate=cut_gate,
+                       due_period=due_period)
         res["audit_identical"] = bool(np.array_equal(aud["ids"], learned["ids"]))
         res["false_stop_rate"] = aud["false_stops"] / max(aud["skipped_sweeps"], 1)
         res["false_stops"] = aud["false_stops"]
@@ -396,6 +400,8 @@ def main(argv=None) -> int:
     e.add_argument("--max-skip", type=int, default=16)
     e.add_argument("--gate", type=float, nargs="*", default=[0.01],
                    help="cut gates: after a round that cut more than this fraction of its clusters, sweep all")
+    e.add_argument("--period", type=int, nargs="*", default=[8],
+                   help="due periods: clusters come due only in rounds whose index is a multiple of it")
     e.add_argument("--report", default=None)
     args = ap.parse_args(argv)
     log = lambda s: print(s, file=sys.stderr, flush=True)
@@ -428,10 +434,11 @@ def main(argv=None) -> int:
             g = make()
             plain = run_mode(g, _lib.SCHEDULE_PLAIN, None, seed, 0.0, 0, 0, 3)
             for sf in args.safety:
-                for gt in args.gate:
-                    r = compare(g, model, seed=seed, safety=sf, max_skip=args.max_skip, cut_gate=gt, plain=plain)
+                for gt, pd in ((gt, pd) for gt in args.gate for pd in args.period):
+                    r = compare(g, model, seed=seed, safety=sf, max_skip=args.max_skip, cut_gate=gt, plain=plain,
+                                due_period=pd)
                     report["eval"].append(r)
-                    log(f"{r['graph']} safety {sf} gate {gt}: speedup {r['speedup']:.3f} "
+                    log(f"{r['graph']} safety {sf} gate {gt} period {pd}: speedup {r['speedup']:.3f} "
                         f"rounds {r['plain']['rounds']} -> {r['learned']['rounds']} cut ratio {r['cut_ratio']:.4f}")
     text = json.dumps(report, indent=1, default=float)
     print(text)

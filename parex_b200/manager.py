@@ -265,12 +265,13 @@ class CudaDeviceManager:
         return {f: getattr(st, f) for f, _ in _lib.Stats._fields_}
 
     def set_schedule(self, mode: int, weights=None, norm=None, safety: float = 0.5, max_skip: int = 16,
-                     trace: bool = False, cut_gate: float = 0.0) -> None:
+                     trace: bool = False, cut_gate: float = 0.0, due_period: int = 0) -> None:
         """Learned sweep schedule (pxr_set_schedule).  weights: MLP_PARAMS bf16
         bit patterns (uint16); norm: 16 means then 16 scales.  cut_gate: after
         a round that cut more than this fraction of its clusters, the next
-        round sweeps every cluster (0: off)."""
-        cfg = _lib.Schedule(mode, 1 if trace else 0, safety, max_skip, cut_gate)
+        round sweeps every cluster (0: off).  due_period > 1: clusters come
+        due only in rounds whose index is a multiple of it."""
+        cfg = _lib.Schedule(mode, 1 if trace else 0, safety, max_skip, cut_gate, due_period)
         w = n = None
         if weights is not None:
             w = np.ascontiguousarray(weights, dtype=np.uint16)

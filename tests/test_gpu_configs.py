@@ -86,7 +86,7 @@ def test_regular22_learned_shipped_model_bit_exact(regular22):
     model = learn.Model.load()
     dm = P.CudaDeviceManager(driver=P.DRIVER_STREAM)
     dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16, trace=True,
-                    cut_gate=0.01)
+                    cut_gate=0.01, due_period=8)
     dm.initialize(g)
     orc = O.Oracle(g.offsets, g.cols, O.MODE_PXR, SC, RW)
     orc.set_potentials(dm.readRandomWalkValues().astype(np.float64))
@@ -111,7 +111,8 @@ def test_regular22_learned_shipped_model_bit_exact(regular22):
     _certified(g.offsets, g.cols, dm, fp)
     # the graph driver runs the same schedule
     gd = P.CudaDeviceManager()
-    gd.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16, cut_gate=0.01)
+    gd.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16, cut_gate=0.01,
+                    due_period=8)
     gd.initialize(g)
     gd.expanderDecomposition()
     np.testing.assert_array_equal(gd.getFinalPartition().clusterIds, ids)

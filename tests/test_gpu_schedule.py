@@ -62,14 +62,14 @@ def test_trace_keeps_plain_result_and_features(name):
     np.testing.assert_array_equal(a.getFinalPartition().clusterIds, b.getFinalPartition().clusterIds)
 
 
-@pytest.mark.parametrize("gate", [0.0, 0.02])
+@pytest.mark.parametrize("gate,period", [(0.0, 0), (0.02, 0), (0.0, 3), (0.02, 3)])
 @pytest.mark.parametrize("name", sorted(GRAPHS))
-def test_scheduled_rounds_match_oracle(name, gate):
+def test_scheduled_rounds_match_oracle(name, gate, period):
     g = GRAPHS[name]()
     model = _random_model(1)
     dm = P.CudaDeviceManager(driver=P.DRIVER_STREAM)
     dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=1.0, max_skip=4, trace=True,
-                    cut_gate=gate)
+                    cut_gate=gate, due_period=period)
     dm.initialize(g)
     orc = O.Oracle(g.offsets, g.cols, O.MODE_PXR)
     orc.set_potentials(dm.readRandomWalkValues().astype(np.float64))
@@ -81,6 +81,7 @@ def test_scheduled_rounds_match_oracle(name, gate):
             break
         assert orc.n_clusters == dm.getNumClusters()
         k_round = np.float32(dm.getNumClusters())
+        a_round = int(dm.stats()["active_vertices"])
         orc.scheduled_round(due)
         dm.iterateRandomWalk()
         dm.computeSweepCuts()
@@ -96,6 +97,10 @@ def test_scheduled_rounds_match_oracle(name, gate):
         if gated:
             assert np.all(rec["skip"] == 0)
             gated_rounds += 1
+        # the due period: outside its rounds no small cluster is due next round
+        held_round = period > 1 and not gated and dm.stats()["rounds"] % period != 0
+        held = held_round & (rec["size"].astype(np.uint64) * 1024 < a_round)
+        assert np.all(rec["skip"][held] >= 1)
         # the product's predictions are the oracle network's on the same features
         sw = rec["origin"] == learn.ORIGIN_SWEPT
         if np.any(sw):
@@ -104,6 +109,7 @@ def test_scheduled_rounds_match_oracle(name, gate):
             r = np.exp2(np.minimum(y.astype(np.float64), 16.0)) - 1.0
             clear = np.abs(r - np.round(r)) > 1e-4          # away from a rounding boundary of floor()
             want = np.zeros(int(np.count_nonzero(sw)), dtype=np.int64) if gated else M.skip_from_prediction(y, 1.0, 4)
+            want = np.where(held[sw], np.maximum(want, 1), want)
             np.testing.assert_array_equal(rec["skip"][sw][clear], want[clear])
         due = (rec["skip"] == 0).astype(np.uint8)
         skipped += int(np.count_nonzero(rec["skip"]))
