@@ -182,8 +182,9 @@ typedef struct {
     uint32_t max_skip;         /* cap on consecutive skipped rounds                                 */
     float cut_gate;            /* a round that cuts more than cut_gate x its clusters skips no sweep
                                   in the next round (every cluster swept, as in PLAIN); 0: off      */
-    uint32_t due_period;       /* > 1: clusters come due only in rounds whose index is a multiple of
-                                  due_period, so small sweeps share rounds; 0 or 1: off           */
+    uint32_t due_period;       /* > 1: clusters under 1/1024 of the active vertices come due only in
+                                  rounds whose index is a multiple of due_period, so their sweeps
+                                  share rounds and the others only walk; 0 or 1: off              */
     uint32_t reserved[2];
 } pxr_schedule;
 

@@ -269,8 +269,9 @@ class CudaDeviceManager:
         """Learned sweep schedule (pxr_set_schedule).  weights: MLP_PARAMS bf16
         bit patterns (uint16); norm: 16 means then 16 scales.  cut_gate: after
         a round that cut more than this fraction of its clusters, the next
-        round sweeps every cluster (0: off).  due_period > 1: clusters come
-        due only in rounds whose index is a multiple of it."""
+        round sweeps every cluster (0: off).  due_period > 1: clusters under
+        1/1024 of the active vertices come due only in rounds whose index is
+        a multiple of it."""
         cfg = _lib.Schedule(mode, 1 if trace else 0, safety, max_skip, cut_gate, due_period)
         w = n = None
         if weights is not None:
