@@ -55,7 +55,7 @@ METRIC = "decomp edges/s"
 UNIT = "edges/s"
 WALK_SEED, GRAPH_SEED, SC, RW = 6582, 1, 0.3, 1e-4
 L2_FLUSH_BYTES = 256 << 20
-SAFETY, MAX_SKIP, CUT_GATE, DUE_PERIOD = 0.25, 16, 0.01, 8
+SAFETY, MAX_SKIP, CUT_GATE, DUE_PERIOD = 0.25, 32, 0.01, 8
 
 
 WORKLOADS = {
@@ -435,7 +435,7 @@ def product_arm(args, rank, world, local_rank):
         if args.row_plan:
             dmx.set_row_plan(*[int(t) for t in args.row_plan.split(",")])
         if form == "learned":
-            dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=SAFETY, max_skip=MAX_SKIP,
+            dmx.set_schedule(P._lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=SAFETY, max_skip=args.max_skip,
                              cut_gate=args.cut_gate, due_period=args.due_period)
         dmx.set_stream(stream.cuda_stream)
         return dmx
@@ -584,7 +584,7 @@ def product_arm(args, rank, world, local_rank):
              "parallelism": (f"{world} ranks, instances split by expected edges" if sharded else "replicas"),
              "job_edges_per_step": job_m}
     if model is not None:
-        extra["learned_schedule"] = {"safety": SAFETY, "max_skip": MAX_SKIP, "cut_gate": args.cut_gate,
+        extra["learned_schedule"] = {"safety": SAFETY, "max_skip": args.max_skip, "cut_gate": args.cut_gate,
                                      "due_period": args.due_period,
                                      "model": "parex_b200/data/stop_predictor.npz"}
     if sharded:
@@ -635,6 +635,7 @@ def main():
     ap.add_argument("--schedule", default="both", choices=["both", "plain", "learned"])
     ap.add_argument("--no-connectivity", dest="connectivity", action="store_false",
                     help="skip the connectivity part of the certificate check")
+    ap.add_argument("--max-skip", type=int, default=MAX_SKIP, help="learned form: cap on consecutive skipped sweeps")
     ap.add_argument("--cut-gate", type=float, default=CUT_GATE,
                     help="learned form: after a round that cut more than this fraction of its clusters, sweep all")
     ap.add_argument("--due-period", type=int, default=DUE_PERIOD,

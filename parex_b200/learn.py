@@ -46,6 +46,10 @@ from .manager import CudaDeviceManager
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(HERE, "data", "stop_predictor.npz")
+# The schedule settings the shipped model is used with (bench, tests, eval):
+# fraction of the predicted skips taken, cap on consecutive skips, the cut
+# gate and the due period of small clusters (pxr_schedule).
+SHIPPED_SCHEDULE = {"safety": 0.25, "max_skip": 32, "cut_gate": 0.01, "due_period": 8}
 F = _lib.MLP_FEATURES
 P = _lib.MLP_PARAMS
 ORIGIN_SWEPT, ORIGIN_CHILD, ORIGIN_CARRIED = 1, 2, 3
@@ -330,7 +334,7 @@ def run_mode(graph, mode: int, model: Model | None, seed: int, safety: float, ma
             "false_stops": st["false_stops"], "ids": fp.clusterIds}
 
 
-def compare(graph, model: Model, seed: int = 6582, safety: float = 0.25, max_skip: int = 16, device: int = 0,
+def compare(graph, model: Model, seed: int = 6582, safety: float = 0.25, max_skip: int = 32, device: int = 0,
             reps: int = 3, audit: bool = True, cut_gate: float = 0.01, plain: dict | None = None,
             due_period: int = 8) -> dict:
     if plain is None:
@@ -389,7 +393,7 @@ def main(argv=None) -> int:
     t.add_argument("--over", type=float, default=4.0)
     t.add_argument("--eval", action="store_true")
     t.add_argument("--safety", type=float, nargs="*", default=[0.25])
-    t.add_argument("--max-skip", type=int, default=16)
+    t.add_argument("--max-skip", type=int, default=32)
     t.add_argument("--report", default=None)
     t.add_argument("--per-round", type=int, default=20000, help="swept clusters sampled per round of a trace")
     t.add_argument("--per-trace", type=int, default=60000, help="samples kept per trace (balances the graphs)")
@@ -397,7 +401,7 @@ def main(argv=None) -> int:
     e = sub.add_parser("eval")
     e.add_argument("--model", default=DEFAULT_MODEL)
     e.add_argument("--safety", type=float, nargs="*", default=[0.25])
-    e.add_argument("--max-skip", type=int, default=16)
+    e.add_argument("--max-skip", type=int, default=32)
     e.add_argument("--gate", type=float, nargs="*", default=[0.01],
                    help="cut gates: after a round that cut more than this fraction of its clusters, sweep all")
     e.add_argument("--period", type=int, nargs="*", default=[8],

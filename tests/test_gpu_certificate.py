@@ -65,7 +65,7 @@ def test_learned_certificates_check(name):
     g = GRAPHS[name]()
     model = learn.Model.load()
     dm = P.CudaDeviceManager()
-    dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16, cut_gate=0.01, due_period=8)
+    dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, **learn.SHIPPED_SCHEDULE)
     dm.initialize(g)
     dm.expanderDecomposition()
     fp = dm.getFinalPartition()

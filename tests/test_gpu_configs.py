@@ -85,8 +85,7 @@ def test_regular22_learned_shipped_model_bit_exact(regular22):
     g = regular22
     model = learn.Model.load()
     dm = P.CudaDeviceManager(driver=P.DRIVER_STREAM)
-    dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16, trace=True,
-                    cut_gate=0.01, due_period=8)
+    dm.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, trace=True, **learn.SHIPPED_SCHEDULE)
     dm.initialize(g)
     orc = O.Oracle(g.offsets, g.cols, O.MODE_PXR, SC, RW)
     orc.set_potentials(dm.readRandomWalkValues().astype(np.float64))
@@ -111,8 +110,7 @@ def test_regular22_learned_shipped_model_bit_exact(regular22):
     _certified(g.offsets, g.cols, dm, fp)
     # the graph driver runs the same schedule
     gd = P.CudaDeviceManager()
-    gd.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, safety=0.25, max_skip=16, cut_gate=0.01,
-                    due_period=8)
+    gd.set_schedule(_lib.SCHEDULE_LEARNED, model.weights, model.norm, **learn.SHIPPED_SCHEDULE)
     gd.initialize(g)
     gd.expanderDecomposition()
     np.testing.assert_array_equal(gd.getFinalPartition().clusterIds, ids)

@@ -33,7 +33,7 @@ HELD_OUT = {
 def _run(g, mode, model):
     dm = P.CudaDeviceManager()
     if mode != _lib.SCHEDULE_PLAIN:
-        dm.set_schedule(mode, model.weights, model.norm, safety=0.25, max_skip=16, cut_gate=0.01, due_period=8)
+        dm.set_schedule(mode, model.weights, model.norm, **learn.SHIPPED_SCHEDULE)
     dm.initialize(g)
     rounds = dm.expanderDecomposition()
     fp = dm.getFinalPartition()
